@@ -1,0 +1,436 @@
+#!/usr/bin/env python
+"""Benchmark: TOD samples/s of the beam-convolution path on B200.
+
+Workload (config 2, plain method on GPU): HEALPix RING nside 1024 float64
+I/Q/U sky, circular Gaussian beam FWHM 30' at beam nside 2048 with a 0.99
+power cut (S = 1512 beam pixels), one 24 h batch of a 100 Hz spin scan
+(8.64e6 samples), one beam entry carrying I, Q and U (spin-2 on), bilinear
+interpolation (``--mode nearest`` for the other mode).
+
+A step is one pass of the fused kernel over the whole batch.
+
+* ``value``: samples/s with the kernel inputs (float32 rotation parameters,
+  boresight longitudes, beam, map) resident in HBM; the step zeroes the
+  float64 (3, B) accumulator and runs the kernel.  Inputs (~1 GB) exceed L2.
+* ``e2e``: the same metric through the public drop-in
+  ``tod_core.beam_tod_batch`` with host numpy inputs (rot_vecs, phi, theta,
+  psis) -> float32 host dict: host parameter preparation, host->device copies,
+  kernel and device->host copy are all inside the timed region.
+* ``cpu_baseline``: the CPU oracle (a C/OpenMP restatement of the reference's
+  Numba kernel) on the host cores, on a bounded sample of the same workload.
+
+``--impl reference`` times that CPU implementation as the benchmark itself
+(rank 0 only), on a bounded sample per step.
+
+Multi-GPU (torchrun): each rank runs its own day of samples (weak scaling, no
+collective on the data path); timings are max-reduced over ranks.
+"""
+
+from __future__ import annotations
+
+import argparse
+import ctypes
+import datetime
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "TOD samples/s, 1 B200: FP64 plain vs mixed/learned-tail at fixed RMS error"
+
+
+def parse_args():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=3)
+    p.add_argument("--warmup", type=int, default=3)
+    p.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    p.add_argument("--mode", choices=["bilinear", "nearest"], default="bilinear")
+    p.add_argument("--samples", type=int, default=8_640_000)
+    p.add_argument("--no-e2e", action="store_true")
+    p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--cpu-seconds", type=float, default=10.0,
+                   help="target CPU time of the bounded CPU-baseline sample")
+    return p.parse_args()
+
+
+# ---------------------------------------------------------------------------
+# distributed plumbing
+# ---------------------------------------------------------------------------
+
+def dist_env():
+    return int(os.environ.get("RANK", 0)), int(os.environ.get("WORLD_SIZE", 1)), int(
+        os.environ.get("LOCAL_RANK", 0))
+
+
+class Dist:
+    def __init__(self):
+        import torch
+
+        self.torch = torch
+        self.rank, self.world, self.local = dist_env()
+        self.pg = None
+        if self.world > 1:
+            import torch.distributed as td
+
+            torch.cuda.set_device(self.local)
+            td.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
+                                  device_id=torch.device("cuda", self.local))
+            self.pg = td
+
+    def barrier(self):
+        if self.pg:
+            self.pg.barrier()
+
+    def max(self, x: float) -> float:
+        if not self.pg:
+            return x
+        t = self.torch.tensor([x], dtype=self.torch.float64, device="cuda")
+        self.pg.all_reduce(t, op=self.pg.ReduceOp.MAX)
+        return float(t.item())
+
+    def close(self):
+        if self.pg:
+            self.pg.destroy_process_group()
+
+
+# ---------------------------------------------------------------------------
+# clocks sampled during the timed region
+# ---------------------------------------------------------------------------
+
+class ClockSampler:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device_index):
+        self.dev = device_index
+        self.proc = None
+        self.lines = []
+        self.thread = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.dev), f"--query-gpu={self.FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except (FileNotFoundError, OSError):
+            self.proc = None
+            return
+        self.thread = threading.Thread(target=self._read, daemon=True)
+        self.thread.start()
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if self.proc is None:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        if self.thread:
+            self.thread.join(timeout=2)
+        sm, smax, reasons = [], 0.0, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                smax = max(smax, float(f[2]))
+            except ValueError:
+                continue
+            for n, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        if not sm:
+            return None
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": smax, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+# ---------------------------------------------------------------------------
+# workload
+# ---------------------------------------------------------------------------
+
+def make_workload(n_samples, rank):
+    from tod_generation_mapbased_beam_b200 import tod_rotations as R
+    from tod_generation_mapbased_beam_b200 import workloads as W
+
+    beam = W.pole_gaussian_beam(30.0, 2048, 0.99, search_fwhm=1.5)
+    # each rank scans its own day (weak scaling): shift the start longitude
+    theta, phi, psi = W.spin_scan(n_samples, 100.0, phi0=0.7 * rank)
+    sky = W.white_sky(1024, seed=1)
+    rot, beta = R.precompute_rotation_vector_batch(beam.ra, beam.dec, phi, theta)
+    psis = -beta + psi
+    return dict(nside=1024, beam=beam, theta=theta, phi=phi, psi=psi, psis=psis, rot=rot, sky=sky)
+
+
+def map_footprint_bytes(wl, itemsize):
+    """Bytes of the map rows the day's scan can touch (the scan sweeps every
+    longitude, so whole rings between the extreme colatitudes +- beam radius)."""
+    nside = wl["nside"]
+    r = wl["beam"].radius + 2 * np.sqrt(4 * np.pi / (12 * nside * nside))
+    th_lo = max(0.0, float(wl["theta"].min()) - r)
+    th_hi = min(np.pi, float(wl["theta"].max()) + r)
+    zs = [np.cos(th_lo), np.cos(th_hi)]
+
+    def first_pix_of_ring(ir):
+        if ir < nside:
+            return 2 * ir * (ir - 1)
+        if ir <= 3 * nside:
+            return 2 * nside * (nside - 1) + (ir - nside) * 4 * nside
+        i2 = 4 * nside - ir
+        return 12 * nside * nside - 2 * i2 * (i2 + 1)
+
+    def ring_of(z):
+        az = abs(z)
+        if az > 2 / 3:
+            ir = int(nside * np.sqrt(3 * (1 - az)))
+            return ir if z > 0 else 4 * nside - ir - 1
+        return int(nside * (2 - 1.5 * z))
+
+    ir0 = max(1, ring_of(zs[0]))
+    ir1 = min(4 * nside - 1, ring_of(zs[1]) + 1)
+    npx = first_pix_of_ring(ir1) + (4 * nside) - first_pix_of_ring(ir0)
+    npx = min(npx, 12 * nside * nside)
+    return npx * 3 * itemsize
+
+
+# ---------------------------------------------------------------------------
+# CPU (oracle) timing
+# ---------------------------------------------------------------------------
+
+def cpu_rate(wl, mode, target_seconds):
+    """Samples/s of the CPU oracle on a bounded sample; returns (rate, n, threads)."""
+    import oracle
+    from tod_generation_mapbased_beam_b200 import tod_rotations as R
+
+    threads = len(os.sched_getaffinity(0))
+    beam = wl["beam"]
+
+    def run(lo, n):
+        sl = slice(lo, lo + n)
+        params = R._rotation_params(wl["rot"][sl], wl["phi"][sl], wl["theta"][sl], wl["psis"][sl])
+        tod = np.zeros((3, n))
+        fn = oracle.gather_accum_fused if mode == "bilinear" else oracle.gather_accum_nearest
+        t0 = time.perf_counter()
+        fn(beam.vec_orig, *params, wl["nside"], wl["sky"], beam.beam_vals, n, beam.S, tod, 1, 2,
+           nthreads=threads)
+        return time.perf_counter() - t0
+
+    run(0, 64)  # page in the library and the map
+    n0 = max(threads * 16, 512)
+    dt = run(1000, n0)
+    n = int(min(len(wl["theta"]) - 2000, max(n0, n0 * target_seconds / max(dt, 1e-6))))
+    best = float("inf")
+    for rep in range(2):
+        best = min(best, run(2000 + rep * 7, n))
+    return n / best, n, threads
+
+
+# ---------------------------------------------------------------------------
+# GPU timing
+# ---------------------------------------------------------------------------
+
+def measured_peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(path) as f:
+            return json.load(f), "measured"
+    except (OSError, ValueError):
+        return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0}, "fallback"
+
+
+def profiled_traffic(mode):
+    """dram bytes per launch recorded by the committed ncu summary, if any."""
+    path = os.path.join(ROOT, "profiles", f"gather_accum_{mode}_config2.md")
+    try:
+        for line in open(path):
+            if line.strip().startswith("dram_bytes_per_launch:"):
+                return float(line.split(":", 1)[1].strip())
+    except OSError:
+        pass
+    return None
+
+
+def run_ours(args, dist):
+    import torch
+
+    from tod_generation_mapbased_beam_b200 import _native, tod_core
+    from tod_generation_mapbased_beam_b200 import tod_rotations as R
+    from tod_generation_mapbased_beam_b200.kernels import boresight_phi_host, make_args
+
+    dev = torch.device("cuda", dist.local)
+    torch.cuda.set_device(dev)
+    wl = make_workload(args.samples, dist.rank)
+    beam = wl["beam"]
+    B, S, nside = args.samples, beam.S, wl["nside"]
+    params_h = R._rotation_params(wl["rot"], wl["phi"], wl["theta"], wl["psis"])
+    bore_h = boresight_phi_host(params_h[3])
+    to = lambda a: torch.from_numpy(np.ascontiguousarray(a)).to(dev)  # noqa: E731
+    params = [to(beam.vec_orig)] + [to(p) for p in params_h]
+    bore = to(bore_h)
+    bv = to(beam.beam_vals)
+    sky = to(wl["sky"])
+    tod = torch.zeros((3, B), dtype=torch.float64, device=dev)
+    interp = _native.BILINEAR if args.mode == "bilinear" else _native.NEAREST
+    cargs = make_args(interp, nside, B, S, 3, 1, 2, params, np.float32, bore, bv, sky, tod)
+    lib = _native.lib()
+    stream = torch.cuda.current_stream(dev)
+
+    def step():
+        tod.zero_()
+        k0.record(stream)
+        _native.check(lib.todgpu_gather_accum(ctypes.byref(cargs), stream.cuda_stream))
+        k1.record(stream)
+
+    k0 = torch.cuda.Event(enable_timing=True)
+    k1 = torch.cuda.Event(enable_timing=True)
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+
+    clocks = ClockSampler(torch.cuda.current_device())
+    clocks.start()
+    time.sleep(0.3)
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    kern_ms = []
+    dist.barrier()
+    torch.cuda.synchronize()
+    ev0.record(stream)
+    for _ in range(args.steps):
+        step()
+        k1.synchronize()
+        kern_ms.append(k0.elapsed_time(k1))
+    ev1.record(stream)
+    torch.cuda.synchronize()
+    dist.barrier()
+    clk = clocks.stop()
+    total_ms = dist.max(ev0.elapsed_time(ev1))
+    kernel_ms = dist.max(statistics.mean(kern_ms))
+    value = B * dist.world * args.steps / (total_ms / 1e3)
+
+    # roofline of the fused kernel (compulsory DRAM bytes per launch)
+    peaks, peak_src = measured_peaks()
+    itemsize = 8
+    bytes_per_launch = (B * (4 * 11 + 8 * 3 * 2) + S * 16 + map_footprint_bytes(wl, itemsize))
+    achieved = bytes_per_launch / (kernel_ms / 1e3) / 1e9
+    traffic = profiled_traffic(args.mode)
+    roofline = {"bound": "hbm", "achieved": round(achieved, 1), "peak": peaks["hbm_gbs"],
+                "unit": "GB/s", "frac": round(achieved / peaks["hbm_gbs"], 4),
+                "traffic": traffic, "peak_source": peak_src,
+                "algorithmic_bytes_per_launch": int(bytes_per_launch),
+                "kernel": "gather_accum_kernel", "kernel_ms": round(kernel_ms, 3),
+                "note": "compute-bound on the FP64 pipe; bytes are the compulsory DRAM traffic"}
+
+    result = {"value": value, "ms_per_step": total_ms / args.steps, "roofline": roofline,
+              "clocks": clk, "gpu_launches": args.steps}
+
+    # end to end through the public drop-in
+    if not args.no_e2e:
+        data = dict(vec_orig=beam.vec_orig, beam_vals=beam.beam_vals, comp_indices=[0, 1, 2],
+                    mp_stacked=wl["sky"])
+
+        def e2e_step():
+            return tod_core.beam_tod_batch(nside, None, data, wl["rot"], wl["phi"], wl["theta"],
+                                           wl["psis"], interp_mode=args.mode)
+
+        for _ in range(args.warmup):
+            e2e_step()
+        torch.cuda.synchronize()
+        dist.barrier()
+        t0 = time.perf_counter()
+        for _ in range(args.steps):
+            out = e2e_step()
+        torch.cuda.synchronize()
+        e2e_s = dist.max(time.perf_counter() - t0)
+        assert out[0].shape == (B,)
+        h2d = B * (4 * 10 + 4)  # float32 rotation parameters + boresight longitude copied per step
+        result["e2e"] = {"value": B * dist.world * args.steps / e2e_s, "unit": "samples/s",
+                         "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(B * 3 * 4),
+                         "api": "tod_core.beam_tod_batch (host numpy in, float32 dict out)"}
+
+    if not args.no_cpu_baseline and dist.rank == 0:
+        rate, n, threads = cpu_rate(wl, args.mode, args.cpu_seconds)
+        result["cpu_baseline"] = {"value": rate, "unit": "samples/s", "cores": threads,
+                                  "kind": "port",
+                                  "sample": f"{n} consecutive samples of the same workload "
+                                            f"(S={S}, nside {nside}), C/OpenMP oracle, best of 2"}
+    return result, B, S
+
+
+def run_reference(args):
+    rank, world, _ = dist_env()
+    if rank != 0:
+        return None
+    wl = make_workload(min(args.samples, 2_000_000), 0)
+    rates = []
+    per_step = max(2.0, 120.0 / max(1, args.steps + args.warmup))
+    for i in range(args.warmup + args.steps):
+        rate, n, threads = cpu_rate(wl, args.mode, min(args.cpu_seconds, per_step))
+        if i >= args.warmup:
+            rates.append((rate, n))
+    value = statistics.mean(r for r, _ in rates)
+    n = rates[-1][1]
+    return {"impl": "reference", "value": value, "threads": threads, "n": n, "S": wl["beam"].S}
+
+
+def main():
+    args = parse_args()
+    base = {"metric": METRIC, "unit": "samples/s", "higher_is_better": True, "steps": args.steps,
+            "warmup": args.warmup, "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic: seeded spin scan, pole-centred Gaussian beam, seeded Gaussian sky"}
+    config = {"workload": f"config2 plain FP64, {args.mode}: nside 1024 f64 I/Q/U sky, 30' FWHM "
+                          f"beam @ nside 2048 0.99 cut, 100 Hz spin scan, one beam entry (I,Q,U; spin-2)",
+              "samples_per_gpu": args.samples, "mode": args.mode,
+              "l2": "inputs larger than L2 (params+map ~1 GB), no flush needed",
+              "params": "float32 reference-typed rotation parameters"}
+    if args.impl == "reference":
+        r = run_reference(args)
+        if r is None:
+            return
+        config["samples_per_gpu"] = r["n"]
+        line = dict(base, impl="reference", value=r["value"], n_gpus=args.gpus,
+                    ms_per_step=r["n"] / r["value"] * 1e3, scaling="weak", config=config,
+                    cpu_baseline={"value": r["value"], "unit": "samples/s", "cores": r["threads"],
+                                  "kind": "port",
+                                  "sample": f"{r['n']} samples per step (S={r['S']}), C/OpenMP "
+                                            "restatement of the reference Numba kernel"},
+                    e2e={"value": r["value"], "unit": "samples/s", "h2d_bytes_per_step": 0,
+                         "d2h_bytes_per_step": 0})
+        print(json.dumps(line))
+        return
+
+    dist = Dist()
+    res, B, S = run_ours(args, dist)
+    if dist.rank == 0:
+        line = dict(base, value=res["value"], n_gpus=dist.world, ms_per_step=res["ms_per_step"],
+                    scaling="weak", config=dict(config, S=S, parallelism=f"samples x{dist.world}"),
+                    roofline=res["roofline"], gpu_launches=res["gpu_launches"],
+                    clocks=res["clocks"])
+        if "e2e" in res:
+            line["e2e"] = res["e2e"]
+        if "cpu_baseline" in res:
+            line["cpu_baseline"] = res["cpu_baseline"]
+        print(json.dumps(line))
+    dist.close()
+
+
+if __name__ == "__main__":
+    main()

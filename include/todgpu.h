@@ -1,0 +1,136 @@
+/*
+ * todgpu.h -- C ABI of the B200 beam-convolution TOD library (libtodgpu.so).
+ *
+ * Plain pointers and sizes only.  Device pointers are CUDA device addresses
+ * on the current device; `stream` is a cudaStream_t passed as void* (NULL =
+ * legacy default stream).  Every entry point returns 0 (TODGPU_OK) or a
+ * negative TODGPU_E* code; todgpu_last_error_string() describes the last
+ * failure of the calling thread.
+ *
+ * Each declaration names the reference interface it replaces
+ * (ArtemBasyrov/tod_generation_mapbased_beam, file:line).
+ */
+#ifndef TODGPU_H
+#define TODGPU_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define TODGPU_ABI_VERSION 1
+
+/* Status codes. */
+#define TODGPU_OK 0
+#define TODGPU_EINVAL -1      /* bad argument (NULL pointer, unknown enum)      */
+#define TODGPU_ENSIDE -2      /* nside outside [1, 8192]                         */
+#define TODGPU_ESHAPE -3      /* B, S or C out of range, c_q/c_u inconsistent    */
+#define TODGPU_EDTYPE -4      /* unsupported dtype combination                   */
+#define TODGPU_ECUDA -5       /* a CUDA runtime call failed                      */
+#define TODGPU_EABI -6        /* abi_version mismatch                            */
+
+/* Interpolation modes (tod_core.py:114-119). */
+#define TODGPU_BILINEAR 0
+#define TODGPU_NEAREST 1
+
+/* Element types. */
+#define TODGPU_F32 0
+#define TODGPU_F64 1
+
+/*
+ * Arguments of one fused gather/accumulate call: one beam entry over a batch
+ * of B samples, accumulating into tod (tod[c*tod_stride + b] += ...).
+ *
+ * params_dtype = TODGPU_F32: vec_orig and the six per-sample parameter arrays
+ *   are float32 and are combined with the reference's operand types (a float32
+ *   recentre step, float64 elsewhere); this is the bit-parity form.
+ *   bore_phi (optional, (B,) float32) holds atan2f(ax_pts[b,1], ax_pts[b,0])
+ *   from the host C library (todgpu_boresight_phi_host): the reference
+ *   computes that longitude with the host libm's float32 atan2, which the
+ *   device's atan2 does not reproduce bit for bit.  When bore_phi is NULL the
+ *   device rounds its float64 atan2 to float32 instead (Q/U may then differ
+ *   from the reference by ~1e-7 relative on some samples).
+ * params_dtype = TODGPU_F64: all float64, bore_phi ignored (precision form).
+ *
+ * map: planar (C, map_stride) of map_dtype, RING order, map_stride >= 12*nside^2.
+ * beam_vals: (S,) float32.  err_count: optional device uint64 counter that
+ * receives the number of (b, s) terms skipped because a stencil pixel fell
+ * outside the map (non-finite pointing); pass NULL to ignore.
+ */
+typedef struct todgpu_gather_args {
+  int32_t abi_version;   /* TODGPU_ABI_VERSION */
+  int32_t interp;        /* TODGPU_BILINEAR or TODGPU_NEAREST */
+  int64_t nside;
+  int64_t B;             /* samples */
+  int64_t S;             /* beam pixels */
+  int64_t C;             /* map components in this entry, 1..4 */
+  int32_t c_q, c_u;      /* Q and U component positions in [0, C), or -1 */
+  int32_t params_dtype;  /* TODGPU_F32 or TODGPU_F64 */
+  int32_t map_dtype;     /* TODGPU_F32 or TODGPU_F64 */
+  const void *vec_orig;  /* (S, 3) */
+  const void *axes;      /* (B, 3) */
+  const void *cos_a;     /* (B,) */
+  const void *sin_a;     /* (B,) */
+  const void *ax_pts;    /* (B, 3) */
+  const void *cos_p;     /* (B,) */
+  const void *sin_p;     /* (B,) */
+  const float *bore_phi; /* (B,) or NULL */
+  const float *beam_vals;/* (S,) */
+  const void *map;       /* (C, map_stride) */
+  int64_t map_stride;
+  double *tod;           /* (C, tod_stride), accumulated in place */
+  int64_t tod_stride;
+  unsigned long long *err_count; /* optional */
+} todgpu_gather_args;
+
+/* Fused rotate -> HEALPix stencil -> spin-2 -> gather -> accumulate.
+ * Replaces tod_bilinear._gather_accum_fused_jit (tod_bilinear.py:205-477)
+ * and tod_nearest._gather_accum_nearest_jit (tod_nearest.py:21-158). */
+int todgpu_gather_accum(const todgpu_gather_args *args, void *stream);
+
+/* Per-(b, s) bilinear stencil of the fused path: pix (4, B*S) int64 and
+ * wgt (4, B*S) float64 with n = b*S + s.  Replaces the split reference path
+ * tod_rotations._rodrigues_jit (tod_rotations.py:33-80) + vec2ang +
+ * get_interp_weights_numba (numba_healpy.py:239-253) used by
+ * tod_bilinear._gather_accum_jit (tod_bilinear.py:41-78).  Only the fields
+ * nside, B, S, params_dtype and the seven parameter pointers of args are read. */
+int todgpu_bilinear_stencils(const todgpu_gather_args *args, int64_t *pix, double *wgt,
+                             void *stream);
+
+/* hp.get_interp_weights in RING order on device arrays theta, phi (N,) f64
+ * -> pix (4, N) int64, wgt (4, N) f64.
+ * Replaces numba_healpy.get_interp_weights_numba (numba_healpy.py:239-253). */
+int todgpu_get_interp_weights(int64_t nside, const double *theta, const double *phi, int64_t N,
+                              int64_t *pix, double *wgt, void *stream);
+
+/* Nearest RING pixel by the 4-candidate rule.
+ * Replaces numba_healpy._ang2pix_ring_jit (numba_healpy.py:642-693). */
+int todgpu_ang2pix(int64_t nside, const double *theta, const double *phi, int64_t N, int64_t *pix,
+                   void *stream);
+
+/* RING pixel centres. Replaces numba_healpy.pix2ang_numba (numba_healpy.py:622-635). */
+int todgpu_pix2ang(int64_t nside, const int64_t *pix, int64_t N, double *theta, double *phi,
+                   void *stream);
+
+/* cos 2d / sin 2d of the spin-2 frame rotation on device arrays (N,).
+ * Replaces tod_bilinear._spin2_cos2d_sin2d_jit (tod_bilinear.py:84-145). */
+int todgpu_spin2(const double *z_pix, const double *sth_pix, const double *phi_pix,
+                 const double *z_pts, const double *sth_pts, const double *phi_pts, int64_t N,
+                 double *c2d, double *s2d, void *stream);
+
+/* HOST function: out[b] = atan2f(ax_pts[3b+1], ax_pts[3b]) with the host C
+ * library, multithreaded.  ax_pts and out are host pointers.  Produces the
+ * boresight longitude the reference kernels compute in float32
+ * (tod_bilinear.py:308, tod_nearest.py:87). */
+int todgpu_boresight_phi_host(const float *ax_pts, int64_t B, float *out, int32_t nthreads);
+
+/* Library introspection. */
+int todgpu_abi_version(void);
+const char *todgpu_last_error_string(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* TODGPU_H */

@@ -1,0 +1,150 @@
+"""GPU parity: the sm_100a kernels against the reference's golden vectors and
+the CPU oracle.
+
+Tolerances (relative to the largest accumulated magnitude of each case):
+  * pixel indices: bit-exact;
+  * float64 TOD, bilinear and nearest: 1e-12;
+  * stencil weights (in [0, 1]): 2e-15 * 4 * nside absolute.  The phi weight
+    is (phi - phi0) / dphi with dphi = 2 pi / (4 nside), so the few-ulp
+    difference between the device's and the host libm's atan2 is amplified by
+    up to 4 nside / (2 pi); 1e-12 holds up to nside ~ 128.
+"""
+
+import numpy as np
+import pytest
+import torch
+
+import oracle
+from conftest import PARAM_KEYS, load_cases, load_flat
+from tod_generation_mapbased_beam_b200 import numba_healpy as nh
+from tod_generation_mapbased_beam_b200 import tod_bilinear, tod_core, tod_nearest
+from tod_generation_mapbased_beam_b200.kernels import bilinear_stencils
+
+pytestmark = pytest.mark.gpu
+
+TOD_RTOL = 1e-12
+
+
+def wgt_atol(nside):
+    return max(1e-12, 2e-15 * 4 * int(nside))
+
+
+def _rel(gpu, ref, base):
+    scale = np.abs(ref - base).max()
+    return np.abs(gpu - ref).max() / max(scale, 1e-300)
+
+
+@pytest.mark.parametrize("mode", ["bilinear", "nearest"])
+@pytest.mark.parametrize("device_tod", [False, True])
+def test_golden_kernels(kernel_case, mode, device_tod):
+    name, g = kernel_case
+    fn = tod_bilinear._gather_accum_fused_jit if mode == "bilinear" else tod_nearest._gather_accum_nearest_jit
+    args = [g[k] for k in PARAM_KEYS]
+    tod = g["tod_init"].copy()
+    if device_tod:
+        tod = torch.from_numpy(tod).cuda()
+    fn(*args, int(g["nside"]), g["mp_stacked"], g["beam_vals"], int(g["B"]), int(g["S"]), tod,
+       int(g["c_q"]), int(g["c_u"]))
+    got = tod.cpu().numpy() if device_tod else tod
+    assert _rel(got, g["tod_" + mode], g["tod_init"]) <= TOD_RTOL
+
+
+def test_golden_stencils(kernel_case):
+    name, g = kernel_case
+    pix, wgt = bilinear_stencils(*[g[k] for k in PARAM_KEYS], int(g["nside"]), int(g["B"]), int(g["S"]))
+    np.testing.assert_array_equal(pix.cpu().numpy(), g["stencil_pix"])
+    np.testing.assert_allclose(wgt.cpu().numpy(), g["stencil_wgt"], rtol=0, atol=wgt_atol(g["nside"]))
+
+
+@pytest.mark.parametrize("case", sorted(load_cases("healpix")))
+def test_golden_healpix(case):
+    g = load_cases("healpix")[case]
+    ns = int(g["nside"])
+    pix, wgt = nh.get_interp_weights_numba(ns, g["theta"], g["phi"])
+    np.testing.assert_array_equal(pix, g["pix"])
+    np.testing.assert_allclose(wgt, g["wgt"], rtol=0, atol=wgt_atol(ns))
+    np.testing.assert_array_equal(nh.ang2pix_ring(ns, g["theta"], g["phi"]), g["ang2pix"])
+    th, ph = nh.pix2ang_numba(ns, g["pix2ang_pix"])
+    np.testing.assert_allclose(th, g["pix2ang_theta"], rtol=0, atol=1e-14)
+    np.testing.assert_array_equal(ph, g["pix2ang_phi"])
+
+
+def test_golden_spin2():
+    g = load_flat("spin2")
+    c2, s2 = tod_bilinear._spin2_cos2d_sin2d_jit(g["z_pix"], g["sth_pix"], g["phi_pix"], g["z_pts"],
+                                                  g["sth_pts"], g["phi_pts"])
+    np.testing.assert_allclose(c2, g["c2d"], rtol=0, atol=1e-12)
+    np.testing.assert_allclose(s2, g["s2d"], rtol=0, atol=1e-12)
+    np.testing.assert_array_equal(c2[:50], 1.0)  # identical points -> identity
+
+
+@pytest.mark.parametrize("tag", ["iqu", "iq", "u"])
+@pytest.mark.parametrize("mode", ["bilinear", "nearest"])
+def test_golden_beam_tod_batch(tag, mode):
+    g = load_flat("core")
+    comps = {"iqu": [0, 1, 2], "iq": [0, 1], "u": [2]}[tag]
+    data = dict(vec_orig=g["vec_orig"], beam_vals=g["beam_vals"], comp_indices=comps,
+                mp_stacked=np.ascontiguousarray(g["maps"][comps]))
+    res = tod_core.beam_tod_batch(int(g["nside"]), list(g["maps"]), data, g["rot_vecs"], g["phi"],
+                                  g["theta"], g["psis"], interp_mode=mode)
+    assert sorted(res) == sorted(comps)
+    ref = g[f"{tag}_{mode}"]
+    for i, c in enumerate(comps):
+        assert res[c].dtype == np.float32 and res[c].shape == ref[i].shape
+        # float64 results agree to 1e-12, so the float32 casts agree to 1 ulp
+        np.testing.assert_array_max_ulp(res[c], ref[i], maxulp=1)
+
+
+def test_beam_tod_batch_rejects_unknown_mode():
+    g = load_flat("core")
+    data = dict(vec_orig=g["vec_orig"], beam_vals=g["beam_vals"], comp_indices=[0],
+                mp_stacked=g["maps"][:1])
+    with pytest.raises(ValueError, match="not available on main branch"):
+        tod_core.beam_tod_batch(16, None, data, g["rot_vecs"], g["phi"], g["theta"], g["psis"],
+                                interp_mode="bicubic")
+
+
+def _config2_like(B, S, nside, seed, dtype=np.float64):
+    """Config-2 shaped inputs: a 30' Gaussian beam near the +z pole in the beam
+    frame and a float32 spin scan recentred onto the sky."""
+    from tod_generation_mapbased_beam_b200 import tod_rotations as R
+
+    rng = np.random.default_rng(seed)
+    r = np.radians(0.65) * np.sqrt(rng.uniform(0, 1, S))
+    a = rng.uniform(0, 2 * np.pi, S)
+    vec = np.stack([np.sin(r) * np.cos(a), np.sin(r) * np.sin(a), np.cos(r)], -1).astype(np.float32)
+    bv = np.exp(-0.5 * (r / np.radians(30 / 60 / 2.355)) ** 2).astype(np.float32)
+    bv /= bv.sum()
+    t = np.arange(B) / 100.0
+    theta = (np.pi / 2 + 0.87 * np.sin(2 * np.pi * t / 60.0)).astype(np.float32)
+    phi = (2 * np.pi * t / 86400.0 + rng.uniform(0, 2 * np.pi)).astype(np.float32) % np.float32(2 * np.pi)
+    psi = (phi.astype(np.float64) + np.pi / 2).astype(np.float32)
+    ra = np.zeros((3, 3))
+    dec = np.full((3, 3), np.pi / 2)
+    rot, beta = R.precompute_rotation_vector_batch(ra, dec, phi, theta)
+    params = R._rotation_params(rot, phi, theta, -beta + psi)
+    mp = rng.standard_normal((3, 12 * nside * nside)).astype(dtype)
+    return vec, bv, params, mp
+
+
+@pytest.mark.parametrize("mode", ["bilinear", "nearest"])
+def test_config2_subset_vs_oracle(mode):
+    """nside 1024 float64 sky, S = 1512 beam pixels, 4096 samples."""
+    B, S, nside = 4096, 1512, 1024
+    vec, bv, params, mp = _config2_like(B, S, nside, seed=5)
+    fn_gpu = tod_bilinear.gather_accum_fused if mode == "bilinear" else tod_nearest.gather_accum_nearest
+    fn_cpu = oracle.gather_accum_fused if mode == "bilinear" else oracle.gather_accum_nearest
+    gpu = torch.zeros((3, B), dtype=torch.float64, device="cuda")
+    fn_gpu(vec, *params, nside, torch.from_numpy(mp).cuda(), bv, B, S, gpu, 1, 2)
+    cpu = np.zeros((3, B))
+    assert fn_cpu(vec, *params, nside, mp, bv, B, S, cpu, 1, 2) == 0
+    assert _rel(gpu.cpu().numpy(), cpu, 0.0) <= TOD_RTOL
+
+
+def test_config2_subset_stencil_pixels_exact():
+    B, S, nside = 512, 1512, 1024
+    vec, bv, params, mp = _config2_like(B, S, nside, seed=6)
+    pix, wgt = bilinear_stencils(vec, *params, nside, B, S)
+    opix, owgt = oracle.bilinear_stencils(vec, *params, nside, B, S)
+    np.testing.assert_array_equal(pix.cpu().numpy(), opix)
+    np.testing.assert_allclose(wgt.cpu().numpy(), owgt, rtol=0, atol=wgt_atol(nside))

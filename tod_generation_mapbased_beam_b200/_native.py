@@ -1,0 +1,131 @@
+"""ctypes binding of libtodgpu.so (the C ABI in include/todgpu.h).
+
+The library is built in-tree by ``tod_generation_mapbased_beam_b200.build``.
+There is no CPU fallback: if the library is missing or CUDA is unavailable,
+every call raises.
+"""
+
+from __future__ import annotations
+
+import ctypes
+import os
+import threading
+
+_PKG = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_PKG, "_lib", "libtodgpu.so")
+
+ABI_VERSION = 1
+OK = 0
+EINVAL, ENSIDE, ESHAPE, EDTYPE, ECUDA, EABI = -1, -2, -3, -4, -5, -6
+BILINEAR, NEAREST = 0, 1
+F32, F64 = 0, 1
+
+_i32 = ctypes.c_int32
+_i64 = ctypes.c_int64
+_p = ctypes.c_void_p
+
+
+class GatherArgs(ctypes.Structure):
+    """Mirror of ``todgpu_gather_args``."""
+
+    _fields_ = [
+        ("abi_version", _i32),
+        ("interp", _i32),
+        ("nside", _i64),
+        ("B", _i64),
+        ("S", _i64),
+        ("C", _i64),
+        ("c_q", _i32),
+        ("c_u", _i32),
+        ("params_dtype", _i32),
+        ("map_dtype", _i32),
+        ("vec_orig", _p),
+        ("axes", _p),
+        ("cos_a", _p),
+        ("sin_a", _p),
+        ("ax_pts", _p),
+        ("cos_p", _p),
+        ("sin_p", _p),
+        ("bore_phi", _p),
+        ("beam_vals", _p),
+        ("map", _p),
+        ("map_stride", _i64),
+        ("tod", _p),
+        ("tod_stride", _i64),
+        ("err_count", _p),
+    ]
+
+
+class TodGpuError(RuntimeError):
+    """A libtodgpu call returned an error status."""
+
+    def __init__(self, code: int, message: str):
+        super().__init__(f"libtodgpu error {code}: {message}")
+        self.code = code
+
+
+_lock = threading.Lock()
+_lib = None
+
+
+def _declare(lib):
+    lib.todgpu_gather_accum.argtypes = [ctypes.POINTER(GatherArgs), _p]
+    lib.todgpu_gather_accum.restype = ctypes.c_int
+    lib.todgpu_bilinear_stencils.argtypes = [ctypes.POINTER(GatherArgs), _p, _p, _p]
+    lib.todgpu_bilinear_stencils.restype = ctypes.c_int
+    lib.todgpu_get_interp_weights.argtypes = [_i64, _p, _p, _i64, _p, _p, _p]
+    lib.todgpu_get_interp_weights.restype = ctypes.c_int
+    lib.todgpu_ang2pix.argtypes = [_i64, _p, _p, _i64, _p, _p]
+    lib.todgpu_ang2pix.restype = ctypes.c_int
+    lib.todgpu_pix2ang.argtypes = [_i64, _p, _i64, _p, _p, _p]
+    lib.todgpu_pix2ang.restype = ctypes.c_int
+    lib.todgpu_spin2.argtypes = [_p] * 6 + [_i64, _p, _p, _p]
+    lib.todgpu_spin2.restype = ctypes.c_int
+    lib.todgpu_boresight_phi_host.argtypes = [_p, _i64, _p, _i32]
+    lib.todgpu_boresight_phi_host.restype = ctypes.c_int
+    lib.todgpu_abi_version.argtypes = []
+    lib.todgpu_abi_version.restype = ctypes.c_int
+    lib.todgpu_last_error_string.argtypes = []
+    lib.todgpu_last_error_string.restype = ctypes.c_char_p
+
+
+def lib():
+    """Load libtodgpu.so once (building it first if it is absent and nvcc is
+    available); raise if that is impossible."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    with _lock:
+        if _lib is not None:
+            return _lib
+        if not os.path.exists(LIB_PATH):
+            from . import build as _build
+
+            _build.build()
+        handle = ctypes.CDLL(LIB_PATH)
+        _declare(handle)
+        if handle.todgpu_abi_version() != ABI_VERSION:
+            raise TodGpuError(EABI, "libtodgpu ABI version mismatch; rebuild the library")
+        _lib = handle
+    return _lib
+
+
+def check(rc: int):
+    if rc != OK:
+        msg = lib().todgpu_last_error_string()
+        raise TodGpuError(rc, msg.decode() if msg else "")
+
+
+def exported_symbols():
+    """Names of the C entry points declared in include/todgpu.h."""
+    return [
+        "todgpu_gather_accum",
+        "todgpu_bilinear_stencils",
+        "todgpu_get_interp_weights",
+        "todgpu_ang2pix",
+        "todgpu_pix2ang",
+        "todgpu_spin2",
+        "todgpu_boresight_phi_host",
+        "todgpu_abi_version",
+        "todgpu_last_error_string",
+    ]

@@ -1,0 +1,162 @@
+"""Kernel-level entry points with the reference's Numba kernel ABI.
+
+``gather_accum`` runs one fused gather/accumulate launch through
+``todgpu_gather_accum``.  Arguments follow ``_gather_accum_fused_jit``
+(tod_bilinear.py:205-222) and ``_gather_accum_nearest_jit``
+(tod_nearest.py:21-38): beam-frame vectors, the six per-sample rotation
+arrays, nside, the planar (C, N) map, beam weights, B, S, the (C, B) float64
+output accumulated in place, and the Q/U component positions.
+
+Inputs may be numpy arrays or torch tensors (CPU or CUDA).  When ``tod`` is a
+numpy array it is copied to the GPU, accumulated there and copied back in
+place, exactly like the reference mutates its argument; CUDA tensors are
+updated in place without a host round trip.
+
+Precision follows the parameter dtype, as it does in the reference (Numba
+specialises the kernel on it): float32 parameters are combined with the
+reference's float32/float64 operand typing (bit-parity form), float64
+parameters give an all-float64 computation.
+"""
+
+from __future__ import annotations
+
+import ctypes
+
+import numpy as np
+import torch
+
+from . import _native
+from ._device import dtype_of, is_tensor, ptr, require_cuda, stream_handle, to_device
+
+_PARAM_NAMES = ("vec_orig", "axes", "cos_a", "sin_a", "ax_pts", "cos_p", "sin_p")
+
+
+def _param_dtype(arrs):
+    dts = {dtype_of(a) for a in arrs}
+    if dts == {np.dtype(np.float32)}:
+        return np.float32
+    if dts == {np.dtype(np.float64)}:
+        return np.float64
+    raise TypeError("vec_orig and the rotation parameter arrays must all be float32 "
+                    f"(reference typing) or all float64; got {sorted(str(d) for d in dts)}")
+
+
+def boresight_phi_host(ax_pts) -> np.ndarray:
+    """atan2f(ax_pts[:,1], ax_pts[:,0]) with the host C library (float32),
+    the boresight longitude the reference kernels compute
+    (tod_bilinear.py:308, tod_nearest.py:87)."""
+    if is_tensor(ax_pts):
+        ax_pts = ax_pts.detach().to("cpu")
+        a = np.ascontiguousarray(ax_pts.numpy(), dtype=np.float32)
+    else:
+        a = np.ascontiguousarray(np.asarray(ax_pts), dtype=np.float32)
+    a = a.reshape(-1, 3)
+    out = np.empty(a.shape[0], dtype=np.float32)
+    _native.check(_native.lib().todgpu_boresight_phi_host(
+        a.ctypes.data_as(ctypes.c_void_p), a.shape[0], out.ctypes.data_as(ctypes.c_void_p), 0))
+    return out
+
+
+def make_args(interp, nside, B, S, C, c_q, c_u, params, pdt, bore_phi, beam, mp, tod,
+              err=None):
+    a = _native.GatherArgs()
+    a.abi_version = _native.ABI_VERSION
+    a.interp = interp
+    a.nside = int(nside)
+    a.B = int(B)
+    a.S = int(S)
+    a.C = int(C)
+    a.c_q = int(c_q)
+    a.c_u = int(c_u)
+    a.params_dtype = _native.F32 if pdt == np.float32 else _native.F64
+    a.map_dtype = _native.F32 if mp.dtype == torch.float32 else _native.F64
+    (a.vec_orig, a.axes, a.cos_a, a.sin_a, a.ax_pts, a.cos_p, a.sin_p) = [ptr(t) for t in params]
+    a.bore_phi = ptr(bore_phi)
+    a.beam_vals = ptr(beam)
+    a.map = ptr(mp)
+    a.map_stride = mp.stride(0)
+    a.tod = ptr(tod)
+    a.tod_stride = tod.stride(0)
+    a.err_count = ptr(err)
+    return a
+
+
+def _map_tensor(mp_stacked):
+    dt = dtype_of(mp_stacked)
+    if dt not in (np.dtype(np.float32), np.dtype(np.float64)):
+        raise TypeError(f"mp_stacked must be float32 or float64, got {dt}")
+    mp = to_device(mp_stacked, dt.type)
+    if mp.dim() != 2:
+        raise ValueError("mp_stacked must be a (C, N) array")
+    return mp
+
+
+def gather_accum(interp, vec_orig, axes, cos_a, sin_a, ax_pts, cos_p, sin_p, nside, mp_stacked,
+                 beam_vals, B, S, tod, c_q=-1, c_u=-1, bore_phi=None, err_count=None):
+    """One fused launch; see the module docstring.  Returns ``tod``."""
+    require_cuda()
+    B = int(B)
+    S = int(S)
+    nside = int(nside)
+    raw = (vec_orig, axes, cos_a, sin_a, ax_pts, cos_p, sin_p)
+    pdt = _param_dtype(raw)
+    shapes = [(S, 3), (B, 3), (B,), (B,), (B, 3), (B,), (B,)]
+    params = [to_device(x, pdt, sh) for x, sh in zip(raw, shapes)]
+    if dtype_of(beam_vals) != np.dtype(np.float32):
+        raise TypeError("beam_vals must be float32 (the reference casts beam weights to float32)")
+    beam = to_device(beam_vals, np.float32, (S,))
+    mp = _map_tensor(mp_stacked)
+    C = mp.shape[0]
+    if pdt == np.float32 and bore_phi is None and B > 0:
+        bore_phi = boresight_phi_host(ax_pts if not is_tensor(ax_pts) else params[4])
+    bphi = to_device(bore_phi, np.float32, (B,)) if (bore_phi is not None and pdt == np.float32) else None
+
+    host_tod = None
+    if is_tensor(tod) and tod.is_cuda:
+        if tod.dtype != torch.float64 or tod.dim() != 2 or tod.stride(1) != 1:
+            raise ValueError("tod must be a float64 (C, B) tensor with unit stride along B")
+        dtod = tod
+    else:
+        host_tod = tod
+        arr = tod.numpy() if is_tensor(tod) else tod
+        if arr.dtype != np.float64 or arr.ndim != 2:
+            raise ValueError("tod must be a float64 (C, B) array")
+        dtod = torch.from_numpy(np.ascontiguousarray(arr)).to(params[0].device)
+    if tuple(dtod.shape) != (C, B):
+        raise ValueError(f"tod has shape {tuple(dtod.shape)}, expected {(C, B)}")
+
+    args = make_args(interp, nside, B, S, C, c_q, c_u, params, pdt, bphi, beam, mp, dtod,
+                     err_count)
+    _native.check(_native.lib().todgpu_gather_accum(ctypes.byref(args), stream_handle()))
+    if host_tod is not None:
+        res = dtod.cpu().numpy()
+        if is_tensor(host_tod):
+            host_tod.copy_(torch.from_numpy(res))
+        else:
+            host_tod[...] = res
+    return tod
+
+
+def bilinear_stencils(vec_orig, axes, cos_a, sin_a, ax_pts, cos_p, sin_p, nside, B, S):
+    """Per-(b, s) bilinear pixels (4, B*S) int64 and weights (4, B*S) float64 of
+    the fused path, as CUDA tensors."""
+    require_cuda()
+    B = int(B)
+    S = int(S)
+    raw = (vec_orig, axes, cos_a, sin_a, ax_pts, cos_p, sin_p)
+    pdt = _param_dtype(raw)
+    shapes = [(S, 3), (B, 3), (B,), (B,), (B, 3), (B,), (B,)]
+    params = [to_device(x, pdt, sh) for x, sh in zip(raw, shapes)]
+    dev = params[0].device
+    pix = torch.empty((4, B * S), dtype=torch.int64, device=dev)
+    wgt = torch.empty((4, B * S), dtype=torch.float64, device=dev)
+    a = _native.GatherArgs()
+    a.abi_version = _native.ABI_VERSION
+    a.nside = int(nside)
+    a.B = B
+    a.S = S
+    a.params_dtype = _native.F32 if pdt == np.float32 else _native.F64
+    (a.vec_orig, a.axes, a.cos_a, a.sin_a, a.ax_pts, a.cos_p, a.sin_p) = [ptr(t) for t in params]
+    _native.check(_native.lib().todgpu_bilinear_stencils(ctypes.byref(a), pix.data_ptr(),
+                                                         wgt.data_ptr(), stream_handle()))
+    return pix, wgt

@@ -1,0 +1,129 @@
+"""Seeded synthetic workloads with the shapes of the reference's benchmark
+configurations (the reference itself ships no data).
+
+* :func:`pole_gaussian_beam` -- a Gaussian beam pixelised at HEALPix pixel
+  centres around the north pole of the beam frame, selected with the
+  reference's power cut (dB threshold, strict ``>``; tod_utils.py:254-297 and
+  sample_based_tod_generation_gridint.py:131-146) and normalised to sum 1.
+* :func:`spin_scan` -- the spin scan theta = pi/2 + 0.87 sin(2 pi t / 60 s),
+  phi drifting 360 deg per day, psi = phi + pi/2, cast to float32 as the
+  reference driver does (gridint.py:277-279).
+* :func:`white_sky` -- seeded Gaussian I/Q/U pixel values (100 uK RMS in I,
+  ~31.6 uK in Q and U).  It stands in for a synfast sky: throughput and
+  parity do not depend on the map content.
+
+Beam-centre convention: (ra, dec) = (0, pi/2), i.e. the beam is centred on
+the beam-frame +z axis, passed through a 3x3 grid whose centre entry is that
+point (tod_rotations.py:251-263 picks the grid centre).
+"""
+
+from __future__ import annotations
+
+import math
+from dataclasses import dataclass
+
+import numpy as np
+
+ARCMIN = math.pi / (180.0 * 60.0)
+
+
+def compute_db_threshold_from_power(beam_vals, power_cut):
+    """dB level keeping ``power_cut`` of the summed beam (tod_utils.py:254-297):
+    sort ascending in dB, suffix sums from the top, last index whose suffix
+    sum still reaches the target."""
+    prof = np.asarray(beam_vals).ravel()
+    target = np.sum(prof) * power_cut
+    with np.errstate(divide="ignore", invalid="ignore"):
+        prof_db = 10 * np.log10(prof)
+    order = np.argsort(prof_db)
+    sorted_db = prof_db[order]
+    suffix = np.cumsum(prof[order][::-1])[::-1]
+    k = np.searchsorted(suffix[::-1], target, side="left")
+    return sorted_db[max(0, len(suffix) - 1 - k)]
+
+
+def select_beam_pixels(beam_vals, power_cut):
+    """Boolean selection ``10 log10(|b| + 1e-30) > threshold``
+    (gridint.py:131-133)."""
+    db = compute_db_threshold_from_power(beam_vals, power_cut)
+    with np.errstate(divide="ignore", invalid="ignore"):
+        return 10 * np.log10(np.abs(beam_vals) + 1e-30) > db
+
+
+def north_cap_pixel_centres(nside, n_rings):
+    """(theta, phi) of every pixel in RING rings 1..n_rings (n_rings < nside)."""
+    th, ph = [], []
+    for i in range(1, n_rings + 1):
+        z = 1.0 - i * i / (3.0 * nside * nside)
+        j = np.arange(4 * i)
+        th.append(np.full(4 * i, math.acos(z)))
+        ph.append((j + 0.5) * (math.pi / (2 * i)))
+    return np.concatenate(th), np.concatenate(ph)
+
+
+@dataclass
+class Beam:
+    vec_orig: np.ndarray   # (S, 3) float32 beam-frame unit vectors
+    beam_vals: np.ndarray  # (S,) float32, sum 1
+    ra: np.ndarray         # (3, 3) beam grid around the centre (only the centre is used)
+    dec: np.ndarray
+    radius: float          # max angular distance of a selected pixel from the centre [rad]
+
+    @property
+    def S(self):
+        return int(self.vec_orig.shape[0])
+
+
+def pole_gaussian_beam(fwhm_arcmin, beam_nside, power_cut, fwhm2_arcmin=None, pol_angle=0.0,
+                       search_fwhm=3.0):
+    """Elliptical Gaussian beam (FWHM along the beam-frame x axis rotated by
+    ``pol_angle``; ``fwhm2_arcmin`` across it) at nside ``beam_nside`` pixel
+    centres within ``search_fwhm`` FWHMs of the pole, power-cut and normalised."""
+    f1 = fwhm_arcmin * ARCMIN
+    f2 = (fwhm2_arcmin if fwhm2_arcmin is not None else fwhm_arcmin) * ARCMIN
+    rmax = search_fwhm * max(f1, f2)
+    pix_size = math.sqrt(4 * math.pi / (12 * beam_nside * beam_nside))
+    n_rings = int(rmax / (pix_size * 0.6)) + 2
+    theta, phi = north_cap_pixel_centres(beam_nside, min(n_rings, beam_nside - 1))
+    keep = theta <= rmax
+    theta, phi = theta[keep], phi[keep]
+    x = theta * np.cos(phi - pol_angle)
+    y = theta * np.sin(phi - pol_angle)
+    s1, s2 = f1 / math.sqrt(8 * math.log(2)), f2 / math.sqrt(8 * math.log(2))
+    b = np.exp(-0.5 * ((x / s1) ** 2 + (y / s2) ** 2))
+    sel = select_beam_pixels(b, power_cut)
+    bv = b[sel].astype(np.float32)
+    bv /= bv.sum()
+    st = np.sin(theta[sel])
+    vec = np.stack([st * np.cos(phi[sel]), st * np.sin(phi[sel]), np.cos(theta[sel])], -1)
+    ra = np.zeros((3, 3))
+    dec = np.full((3, 3), math.pi / 2)
+    return Beam(vec.astype(np.float32), bv, ra, dec, float(theta[sel].max()))
+
+
+def spin_scan(n_samples, rate_hz, t0=0.0, phi0=0.0):
+    """Float32 (theta, phi, psi) of the spin scan."""
+    t = t0 + np.arange(n_samples, dtype=np.float64) / rate_hz
+    theta = math.pi / 2 + 0.87 * np.sin(2 * math.pi * t / 60.0)
+    phi = np.mod(phi0 + 2 * math.pi * t / 86400.0, 2 * math.pi)
+    psi = phi + math.pi / 2
+    return theta.astype(np.float32), phi.astype(np.float32), psi.astype(np.float32)
+
+
+def white_sky(nside, seed, dtype=np.float64):
+    """(3, 12 nside^2) seeded Gaussian I/Q/U in K (I RMS 100 uK, Q/U ~31.6 uK)."""
+    rng = np.random.default_rng(seed)
+    npix = 12 * nside * nside
+    out = np.empty((3, npix), dtype=dtype)
+    for c, rms in enumerate((100e-6, 31.6e-6, 31.6e-6)):
+        out[c] = rng.standard_normal(npix) * rms
+    return out
+
+
+def config2(n_samples=8_640_000, seed=1):
+    """Plain method on GPU (config 2): nside 1024 float64 sky, 30' FWHM
+    circular beam at beam nside 2048 with a 0.99 power cut, 100 Hz spin scan."""
+    beam = pole_gaussian_beam(30.0, 2048, 0.99, search_fwhm=1.5)  # S = 1512
+    theta, phi, psi = spin_scan(n_samples, 100.0)
+    sky = white_sky(1024, seed)
+    return dict(nside=1024, beam=beam, theta=theta, phi=phi, psi=psi, sky=sky)

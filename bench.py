@@ -57,6 +57,8 @@ def parse_args():
     p.add_argument("--samples", type=int, default=8_640_000)
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--no-tables", action="store_true",
+                   help="evaluate ring data and spin-2 angles directly (A/B comparison)")
     p.add_argument("--cpu-seconds", type=float, default=10.0,
                    help="target CPU time of the bounded CPU-baseline sample")
     return p.parse_args()
@@ -273,7 +275,8 @@ def run_ours(args, dist):
 
     from tod_generation_mapbased_beam_b200 import _native, tod_core
     from tod_generation_mapbased_beam_b200 import tod_rotations as R
-    from tod_generation_mapbased_beam_b200.kernels import boresight_phi_host, make_args
+    from tod_generation_mapbased_beam_b200.kernels import (beam_reach, boresight_phi_host, make_args,
+                                                           ring_table)
 
     dev = torch.device("cuda", dist.local)
     torch.cuda.set_device(dev)
@@ -289,7 +292,9 @@ def run_ours(args, dist):
     sky = to(wl["sky"])
     tod = torch.zeros((3, B), dtype=torch.float64, device=dev)
     interp = _native.BILINEAR if args.mode == "bilinear" else _native.NEAREST
-    cargs = make_args(interp, nside, B, S, 3, 1, 2, params, np.float32, bore, bv, sky, tod)
+    table = None if args.no_tables else ring_table(nside, beam_reach(beam.vec_orig, nside), dev)
+    cargs = make_args(interp, nside, B, S, 3, 1, 2, params, np.float32, bore, bv, sky, tod,
+                      table=table)
     lib = _native.lib()
     stream = torch.cuda.current_stream(dev)
 

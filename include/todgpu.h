@@ -13,6 +13,7 @@
 #ifndef TODGPU_H
 #define TODGPU_H
 
+#include <stddef.h>
 #include <stdint.h>
 
 #ifdef __cplusplus
@@ -33,6 +34,10 @@ extern "C" {
 /* Interpolation modes (tod_core.py:114-119). */
 #define TODGPU_BILINEAR 0
 #define TODGPU_NEAREST 1
+
+/* Flags (todgpu_gather_args.flags). */
+#define TODGPU_FLAG_NO_TABLES 1 /* ignore ring_table: evaluate every stencil ring and spin-2
+                                   angle directly (same results, slower) */
 
 /* Element types. */
 #define TODGPU_F32 0
@@ -82,6 +87,10 @@ typedef struct todgpu_gather_args {
   double *tod;           /* (C, tod_stride), accumulated in place */
   int64_t tod_stride;
   unsigned long long *err_count; /* optional */
+  int32_t flags;         /* TODGPU_FLAG_* */
+  int32_t reserved;
+  const void *ring_table;/* optional: table built by todgpu_ring_table_build for this
+                            nside; NULL evaluates ring data and spin-2 angles directly */
 } todgpu_gather_args;
 
 /* Fused rotate -> HEALPix stencil -> spin-2 -> gather -> accumulate.
@@ -124,6 +133,19 @@ int todgpu_spin2(const double *z_pix, const double *sth_pix, const double *phi_p
  * boresight longitude the reference kernels compute in float32
  * (tod_bilinear.py:308, tod_nearest.py:87). */
 int todgpu_boresight_phi_host(const float *ax_pts, int64_t B, float *out, int32_t nthreads);
+
+/* Ring table: per-ring data of the RING scheme for one nside (ring z, acos z,
+ * layout) and, for footprints of angular radius up to `reach` (radians), the
+ * spin-2 table slots each ring needs.  todgpu_gather_accum reads it through
+ * args->ring_table (lookups only; it is never written by the gather).  The
+ * caller allocates `todgpu_ring_table_bytes(nside)` bytes of device memory
+ * (16-byte aligned) and builds it once per (nside, reach) on `stream`.  A
+ * beam wider than `reach` (its radius plus 4/nside) still runs, with the
+ * spin-2 angles evaluated directly.  No counterpart in the reference, whose
+ * kernels recompute ring data per evaluation (numba_healpy.py:73-114) and
+ * cache spin-2 angles per sample (tod_bilinear.py:151-199). */
+size_t todgpu_ring_table_bytes(int64_t nside);
+int todgpu_ring_table_build(int64_t nside, double reach, void *table, size_t bytes, void *stream);
 
 /* Library introspection. */
 int todgpu_abi_version(void);

@@ -19,6 +19,7 @@ OK = 0
 EINVAL, ENSIDE, ESHAPE, EDTYPE, ECUDA, EABI = -1, -2, -3, -4, -5, -6
 BILINEAR, NEAREST = 0, 1
 F32, F64 = 0, 1
+FLAG_NO_TABLES = 1
 
 _i32 = ctypes.c_int32
 _i64 = ctypes.c_int64
@@ -53,6 +54,9 @@ class GatherArgs(ctypes.Structure):
         ("tod", _p),
         ("tod_stride", _i64),
         ("err_count", _p),
+        ("flags", _i32),
+        ("reserved", _i32),
+        ("ring_table", _p),
     ]
 
 
@@ -83,6 +87,10 @@ def _declare(lib):
     lib.todgpu_spin2.restype = ctypes.c_int
     lib.todgpu_boresight_phi_host.argtypes = [_p, _i64, _p, _i32]
     lib.todgpu_boresight_phi_host.restype = ctypes.c_int
+    lib.todgpu_ring_table_bytes.argtypes = [_i64]
+    lib.todgpu_ring_table_bytes.restype = ctypes.c_size_t
+    lib.todgpu_ring_table_build.argtypes = [_i64, ctypes.c_double, _p, ctypes.c_size_t, _p]
+    lib.todgpu_ring_table_build.restype = ctypes.c_int
     lib.todgpu_abi_version.argtypes = []
     lib.todgpu_abi_version.restype = ctypes.c_int
     lib.todgpu_last_error_string.argtypes = []
@@ -102,7 +110,7 @@ def lib():
             from . import build as _build
 
             _build.build()
-        handle = ctypes.CDLL(LIB_PATH)
+        handle = ctypes.CDLL(os.environ.get("TODGPU_LIBRARY", LIB_PATH))
         _declare(handle)
         if handle.todgpu_abi_version() != ABI_VERSION:
             raise TodGpuError(EABI, "libtodgpu ABI version mismatch; rebuild the library")
@@ -126,6 +134,8 @@ def exported_symbols():
         "todgpu_pix2ang",
         "todgpu_spin2",
         "todgpu_boresight_phi_host",
+        "todgpu_ring_table_bytes",
+        "todgpu_ring_table_build",
         "todgpu_abi_version",
         "todgpu_last_error_string",
     ]

@@ -121,121 +121,127 @@ __device__ __forceinline__ double hp_ring_z(long long nside, long long ir) {
   }
 }
 
-// 4-neighbour bilinear stencil of a query (z clamped to [-1,1], phi in
-// [0, 2pi)): pixels, weights and each neighbour's ring z and longitude.
-struct Stencil {
-  long long p[4];
-  double w[4];
-  double zn[4];
-  double phin[4];
+// Everything the stencil needs about one ring.  `ta` is acos(z).
+struct RingData {
+  long long n, first;
+  double phi0, dphi, z, ta;
 };
 
-__device__ __forceinline__ void hp_stencil(long long nside, double z, double phi_w, long long npix,
-                                           Stencil& st) {
+// Ring provider that derives every ring quantity on the fly.
+struct DirectRings {
+  long long nside, npix;
+  __device__ __forceinline__ RingData operator()(long long ir) const {
+    RingInfo r = hp_ring_info(nside, ir, npix);
+    RingData d;
+    d.n = r.n;
+    d.first = r.first;
+    d.phi0 = r.phi0;
+    d.dphi = r.dphi;
+    d.z = hp_ring_z(nside, ir);
+    d.ta = acos(d.z);
+    return d;
+  }
+  __device__ __forceinline__ double sth(long long, const RingData& d) const { return sqrt(max0(1.0 - d.z * d.z)); }
+};
+
+// Ring provider for the nearest rule, which needs no acos of the ring z.
+struct DirectRingsNoAcos {
+  long long nside, npix;
+  __device__ __forceinline__ RingData operator()(long long ir) const {
+    RingInfo r = hp_ring_info(nside, ir, npix);
+    RingData d;
+    d.n = r.n;
+    d.first = r.first;
+    d.phi0 = r.phi0;
+    d.dphi = r.dphi;
+    d.z = hp_ring_z(nside, ir);
+    d.ta = 0.0;
+    return d;
+  }
+  __device__ __forceinline__ double sth(long long, const RingData& d) const { return sqrt(max0(1.0 - d.z * d.z)); }
+};
+
+// 4-neighbour bilinear stencil of a query (z clamped to [-1,1], phi in
+// [0, 2pi)).  For each neighbour k = 0..3, in the reference's order, calls
+//   visit(k, pixel, weight, ring, in_ring_index, ring_length, ring_z, pixel_phi)
+// The in-ring index equals the ring length n when the reference's phi modulo
+// rounds up to n: the pixel then spills into the next ring, exactly as in the
+// reference (numba_healpy.py:453-471).
+template <class Rings, class Visit>
+__device__ __forceinline__ void hp_stencil(long long nside, double z, double phi_w, const Rings& rings,
+                                           Visit&& visit) {
   const long long ir_above = hp_ring_above(nside, z);
   const long long ir_below = wrap_add(ir_above, 1);
   if (ir_above == 0) {
     // North of ring 1: ring 1 pair plus the opposite pair of ring 1.
-    RingInfo ra = hp_ring_info(nside, 1, npix);
-    double tw = py_fmod_pos((phi_w - ra.phi0) / ra.dphi, (double)ra.n);
-    long long ip = py_int(tw);
-    double frac = tw - (double)ip;
-    long long ip2 = py_imod(wrap_add(ip, 1), ra.n);
-    long long o1 = py_imod(wrap_add(ip, 2), ra.n), o2 = py_imod(ip2 + 2, ra.n);
-    st.p[0] = ra.first + o1;
-    st.p[1] = ra.first + o2;
-    st.p[2] = wrap_add(ra.first, ip);
-    st.p[3] = ra.first + ip2;
-    double za = hp_ring_z(nside, 1);
-    double ta = acos(za);
-    double theta = acos(z);
-    double wt = theta / ta;
-    double nf = (1.0 - wt) * 0.25;
-    st.w[0] = nf;
-    st.w[1] = nf;
-    st.w[2] = (1.0 - frac) * wt + nf;
-    st.w[3] = frac * wt + nf;
-    st.zn[0] = st.zn[1] = st.zn[2] = st.zn[3] = za;
-    st.phin[0] = ra.phi0 + (double)o1 * ra.dphi;
-    st.phin[1] = ra.phi0 + (double)o2 * ra.dphi;
-    st.phin[2] = ra.phi0 + (double)ip * ra.dphi;
-    st.phin[3] = ra.phi0 + (double)ip2 * ra.dphi;
+    const RingData ra = rings(1);
+    const double tw = py_fmod_pos((phi_w - ra.phi0) / ra.dphi, (double)ra.n);
+    const long long ip = py_int(tw);
+    const double frac = tw - (double)ip;
+    const long long ip2 = py_imod(wrap_add(ip, 1), ra.n);
+    const long long o1 = py_imod(wrap_add(ip, 2), ra.n), o2 = py_imod(ip2 + 2, ra.n);
+    const double theta = acos(z);
+    const double wt = theta / ra.ta;
+    const double nf = (1.0 - wt) * 0.25;
+    visit(0, ra.first + o1, nf, 1LL, o1, ra.n, ra.z, ra.phi0 + (double)o1 * ra.dphi);
+    visit(1, ra.first + o2, nf, 1LL, o2, ra.n, ra.z, ra.phi0 + (double)o2 * ra.dphi);
+    visit(2, wrap_add(ra.first, ip), (1.0 - frac) * wt + nf, 1LL, ip, ra.n, ra.z, ra.phi0 + (double)ip * ra.dphi);
+    visit(3, ra.first + ip2, frac * wt + nf, 1LL, ip2, ra.n, ra.z, ra.phi0 + (double)ip2 * ra.dphi);
   } else if (ir_below == 4 * nside) {
     // South of the last ring: last-ring pair plus its opposite pair.
     const long long ir_last = 4 * nside - 1;
-    RingInfo ra = hp_ring_info(nside, ir_last, npix);
-    double tw = py_fmod_pos((phi_w - ra.phi0) / ra.dphi, (double)ra.n);
-    long long ip = py_int(tw);
-    double frac = tw - (double)ip;
-    long long ip2 = py_imod(wrap_add(ip, 1), ra.n);
-    long long o1 = py_imod(wrap_add(ip, 2), ra.n), o2 = py_imod(ip2 + 2, ra.n);
-    st.p[0] = wrap_add(ra.first, ip);
-    st.p[1] = ra.first + ip2;
-    st.p[2] = ra.first + o1;
-    st.p[3] = ra.first + o2;
-    double za = hp_ring_z(nside, ir_last);
-    double ta = acos(za);
-    double theta = acos(z);
-    double ws = (theta - ta) / (kPi - ta);
-    double sf = ws * 0.25;
-    st.w[0] = (1.0 - frac) * (1.0 - ws) + sf;
-    st.w[1] = frac * (1.0 - ws) + sf;
-    st.w[2] = sf;
-    st.w[3] = sf;
-    st.zn[0] = st.zn[1] = st.zn[2] = st.zn[3] = za;
-    st.phin[0] = ra.phi0 + (double)ip * ra.dphi;
-    st.phin[1] = ra.phi0 + (double)ip2 * ra.dphi;
-    st.phin[2] = ra.phi0 + (double)o1 * ra.dphi;
-    st.phin[3] = ra.phi0 + (double)o2 * ra.dphi;
+    const RingData ra = rings(ir_last);
+    const double tw = py_fmod_pos((phi_w - ra.phi0) / ra.dphi, (double)ra.n);
+    const long long ip = py_int(tw);
+    const double frac = tw - (double)ip;
+    const long long ip2 = py_imod(wrap_add(ip, 1), ra.n);
+    const long long o1 = py_imod(wrap_add(ip, 2), ra.n), o2 = py_imod(ip2 + 2, ra.n);
+    const double theta = acos(z);
+    const double ws = (theta - ra.ta) / (kPi - ra.ta);
+    const double sf = ws * 0.25;
+    visit(0, wrap_add(ra.first, ip), (1.0 - frac) * (1.0 - ws) + sf, ir_last, ip, ra.n, ra.z,
+          ra.phi0 + (double)ip * ra.dphi);
+    visit(1, ra.first + ip2, frac * (1.0 - ws) + sf, ir_last, ip2, ra.n, ra.z, ra.phi0 + (double)ip2 * ra.dphi);
+    visit(2, ra.first + o1, sf, ir_last, o1, ra.n, ra.z, ra.phi0 + (double)o1 * ra.dphi);
+    visit(3, ra.first + o2, sf, ir_last, o2, ra.n, ra.z, ra.phi0 + (double)o2 * ra.dphi);
   } else {
-    double za = hp_ring_z(nside, ir_above);
-    double zb = hp_ring_z(nside, ir_below);
-    double ta = acos(za);
-    double tb = acos(zb);
-    double theta = acos(z);
-    double wb = (theta - ta) / (tb - ta);
-    double wa = 1.0 - wb;
-    RingInfo ra = hp_ring_info(nside, ir_above, npix);
+    const RingData ra = rings(ir_above);
+    const RingData rb = rings(ir_below);
+    const double theta = acos(z);
+    const double wb = (theta - ra.ta) / (rb.ta - ra.ta);
+    const double wa = 1.0 - wb;
     double tw = py_fmod_pos((phi_w - ra.phi0) / ra.dphi, (double)ra.n);
-    long long ia = py_int(tw);
-    double fa = tw - (double)ia;
-    long long ia1 = py_imod(wrap_add(ia, 1), ra.n);
-    st.p[0] = wrap_add(ra.first, ia);
-    st.p[1] = ra.first + ia1;
-    st.w[0] = wa * (1.0 - fa);
-    st.w[1] = wa * fa;
-    RingInfo rb = hp_ring_info(nside, ir_below, npix);
+    const long long ia = py_int(tw);
+    const double fa = tw - (double)ia;
+    const long long ia1 = py_imod(wrap_add(ia, 1), ra.n);
+    visit(0, wrap_add(ra.first, ia), wa * (1.0 - fa), ir_above, ia, ra.n, ra.z, ra.phi0 + (double)ia * ra.dphi);
+    visit(1, ra.first + ia1, wa * fa, ir_above, ia1, ra.n, ra.z, ra.phi0 + (double)ia1 * ra.dphi);
     tw = py_fmod_pos((phi_w - rb.phi0) / rb.dphi, (double)rb.n);
-    long long ib = py_int(tw);
-    double fb = tw - (double)ib;
-    long long ib1 = py_imod(wrap_add(ib, 1), rb.n);
-    st.p[2] = wrap_add(rb.first, ib);
-    st.p[3] = rb.first + ib1;
-    st.w[2] = wb * (1.0 - fb);
-    st.w[3] = wb * fb;
-    st.zn[0] = za;
-    st.zn[1] = za;
-    st.zn[2] = zb;
-    st.zn[3] = zb;
-    st.phin[0] = ra.phi0 + (double)ia * ra.dphi;
-    st.phin[1] = ra.phi0 + (double)ia1 * ra.dphi;
-    st.phin[2] = rb.phi0 + (double)ib * rb.dphi;
-    st.phin[3] = rb.phi0 + (double)ib1 * rb.dphi;
+    const long long ib = py_int(tw);
+    const double fb = tw - (double)ib;
+    const long long ib1 = py_imod(wrap_add(ib, 1), rb.n);
+    visit(2, wrap_add(rb.first, ib), wb * (1.0 - fb), ir_below, ib, rb.n, rb.z, rb.phi0 + (double)ib * rb.dphi);
+    visit(3, rb.first + ib1, wb * fb, ir_below, ib1, rb.n, rb.z, rb.phi0 + (double)ib1 * rb.dphi);
   }
 }
 
 // Nearest pixel by the reference's 4-candidate rule (two rings bracketing z,
 // two phi slots per ring, maximum cos distance; ties keep the first).
 // z and sin_th are used as given (the nearest kernel passes the unnormalised
-// rotated z and sqrt(vx^2+vy^2)).
+// rotated z and sqrt(vx^2+vy^2)).  `ring_sth(ir, d)` returns
+// sqrt(max(0, 1 - z_ring^2)) for ring data d.
 struct Nearest {
   long long pix;
+  long long ring;
+  long long ip;  // in-ring index, always in [0, n)
+  long long n;   // pixels in the chosen ring
   double zc;
   double phic;
 };
 
+template <class Rings>
 __device__ __forceinline__ Nearest hp_nearest(long long nside, double z, double sin_th, double phi_w,
-                                              long long npix) {
+                                              const Rings& rings) {
   long long ir_above = hp_ring_above(nside, z);
   if (ir_above < 1)
     ir_above = 1;
@@ -243,25 +249,30 @@ __device__ __forceinline__ Nearest hp_nearest(long long nside, double z, double 
     ir_above = 4 * nside - 2;
   Nearest best;
   best.pix = 0;
+  best.ring = 0;
+  best.ip = 0;
+  best.n = 1;
   best.zc = 0.0;
   best.phic = 0.0;
   double best_cos = -2.0;
 #pragma unroll
   for (int g = 0; g < 2; ++g) {
     const long long ir = ir_above + g;
-    RingInfo r = hp_ring_info(nside, ir, npix);
-    double zc = hp_ring_z(nside, ir);
-    double szc = sqrt(max0(1.0 - zc * zc));
-    long long ipb = py_imod(py_int(phi_w * (double)r.n / kTwoPi), r.n);
+    const RingData r = rings(ir);
+    const double szc = rings.sth(ir, r);
+    const long long ipb = py_imod(py_int(phi_w * (double)r.n / kTwoPi), r.n);
 #pragma unroll
     for (int t = 0; t < 2; ++t) {
-      long long ip = (t == 0) ? ipb : py_imod(ipb + 1, r.n);
-      double phic = r.phi0 + (double)ip * r.dphi;
-      double cosd = sin_th * szc * cos(phi_w - phic) + z * zc;
+      const long long ip = (t == 0) ? ipb : py_imod(ipb + 1, r.n);
+      const double phic = r.phi0 + (double)ip * r.dphi;
+      const double cosd = sin_th * szc * cos(phi_w - phic) + z * r.z;
       if (cosd > best_cos) {
         best_cos = cosd;
         best.pix = r.first + ip;
-        best.zc = zc;
+        best.ring = ir;
+        best.ip = ip;
+        best.n = r.n;
+        best.zc = r.z;
         best.phic = phic;
       }
     }

@@ -1,18 +1,26 @@
 // tod_gather.cu -- fused beam-convolution TOD kernels for B200 (sm_100a) and
 // the C ABI declared in include/todgpu.h.
 //
-// Work decomposition: a persistent grid of 256-thread CTAs walks the sample
-// batch in tiles of 8 consecutive samples; each warp owns one sample of the
-// tile and its 32 lanes stride over the beam pixels, so the per-sample
-// rotation scalars are warp-uniform and every lane runs the full per-pixel
-// pipeline (rotate -> atan2/clamp -> RING stencil -> spin-2 -> gather ->
-// FP64 accumulate).  Lane partial sums are combined with warp shuffles and
-// lane 0 adds the result into tod[c, b]; each sample has exactly one writer,
-// so no atomics are needed and repeated runs are bit-reproducible.
-//
-// The beam (unit vectors + weights) is staged in shared memory in chunks of
-// kChunk pixels as {vx, vy, vz, w} records; when the whole beam fits it is
-// loaded once per CTA and stays resident for every tile.
+// Work decomposition ("footprint" kernel): a persistent grid of 256-thread
+// CTAs walks the samples; a CTA takes one sample at a time and
+//   1. rotates the beam's centre direction with the sample's rotation to get
+//      the footprint centre, and derives the window of RING rings the
+//      footprint (beam radius + stencil reach) can touch;
+//   2. tabulates per window ring (in shared memory) the ring layout, ring z,
+//      acos(ring z) and sqrt(1 - z^2), and the longitude range of ring pixels
+//      inside the footprint;
+//   3. tabulates cos 2d / sin 2d of the spin-2 frame rotation for every ring
+//      pixel in the footprint once (a stencil pixel is shared by ~16 (beam
+//      pixel, neighbour) pairs of a sample);
+//   4. strides its threads over the beam pixels: rotate -> atan2/clamp ->
+//      RING stencil (ring data from the window) -> spin-2 (from the table) ->
+//      gather -> FP64 accumulate;
+//   5. reduces the per-thread sums in a fixed order and adds them into
+//      tod[c, b] (one writer per sample: no atomics, bit-reproducible runs).
+// Table values are produced by the same functions on the same inputs as
+// direct evaluation, so they are bit-identical to it; any lookup outside the
+// window (or a footprint too large for the tables) falls back to direct
+// evaluation.  The window therefore only decides speed, never results.
 //
 // Compiled with -fmad=false: the pixel decisions and the FP64 accumulation
 // reproduce the reference's uncontracted arithmetic.
@@ -32,10 +40,8 @@
 
 namespace todgpu {
 
-constexpr int kWarps = 8;
-constexpr int kThreads = kWarps * 32;
-constexpr int kChunkF32 = 4096;  // beam pixels per shared-memory chunk (16 B each)
-constexpr int kChunkF64 = 2048;  // (32 B each)
+constexpr int kRingCap = 192;   // rings per footprint window
+constexpr int kTabCapDefault = 2048;  // spin-2 table slots per sample (32 KB)
 constexpr long long kMaxNside = 16384;
 
 thread_local std::string g_last_error;
@@ -49,17 +55,11 @@ static int cuda_fail(cudaError_t e, const char* what) {
   return fail(TODGPU_ECUDA, std::string(what) + ": " + cudaGetErrorString(e));
 }
 
-struct BeamF32 {
-  float x, y, z, w;
-};
-struct BeamF64 {
-  double x, y, z;
-  float w, pad;
-};
-
 struct KArgs {
   long long nside, npix, B, S;
   int C, c_q, c_u;
+  int tab_cap;               // spin-2 table slots in shared memory
+  const void* ring_table;    // RingRec[4 nside] or nullptr
   const void* vec;
   const void* axes;
   const void* cos_a;
@@ -74,19 +74,6 @@ struct KArgs {
   double* tod;
   long long tod_stride;
   unsigned long long* err;
-};
-
-template <bool P64>
-struct ParamTraits;
-template <>
-struct ParamTraits<false> {
-  using Beam = BeamF32;
-  static constexpr int kChunk = kChunkF32;
-};
-template <>
-struct ParamTraits<true> {
-  using Beam = BeamF64;
-  static constexpr int kChunk = kChunkF64;
 };
 
 template <bool P64>
@@ -113,6 +100,11 @@ __device__ __forceinline__ SampleRot load_rot(const KArgs& a, long long b) {
     r.fkz = ax[2];
     r.fca = static_cast<const float*>(a.cos_a)[b];
     r.fsa = static_cast<const float*>(a.sin_a)[b];
+    r.kx = (double)r.fkx;
+    r.ky = (double)r.fky;
+    r.kz = (double)r.fkz;
+    r.ca = (double)r.fca;
+    r.sa = (double)r.fsa;
     r.px = (double)pt[0];
     r.py = (double)pt[1];
     r.pz = (double)pt[2];
@@ -147,34 +139,17 @@ __device__ __forceinline__ void load_boresight(const KArgs& a, long long b, doub
   if (phi < 0.0) phi += kTwoPi;
 }
 
+// Rotated beam pixel s of the sample.
 template <bool P64>
-__device__ __forceinline__ void stage_beam(const KArgs& a, typename ParamTraits<P64>::Beam* sm,
-                                           long long s0, int n) {
-  for (int i = threadIdx.x; i < n; i += blockDim.x) {
-    const long long s = s0 + i;
-    if constexpr (P64) {
-      const double* v = static_cast<const double*>(a.vec) + 3 * s;
-      BeamF64 e;
-      e.x = v[0];
-      e.y = v[1];
-      e.z = v[2];
-      e.w = a.beam[s];
-      e.pad = 0.f;
-      sm[i] = e;
-    } else {
-      const float* v = static_cast<const float*>(a.vec) + 3 * s;
-      sm[i] = BeamF32{v[0], v[1], v[2], a.beam[s]};
-    }
+__device__ __forceinline__ void rotate_pixel(const KArgs& a, const SampleRot& r, long long s, double& vx,
+                                             double& vy, double& vz) {
+  if constexpr (P64) {
+    const double* v = static_cast<const double*>(a.vec) + 3 * s;
+    rot_f64(r, __ldg(v), __ldg(v + 1), __ldg(v + 2), vx, vy, vz);
+  } else {
+    const float* v = static_cast<const float*>(a.vec) + 3 * s;
+    rot_ref32(r, __ldg(v), __ldg(v + 1), __ldg(v + 2), vx, vy, vz);
   }
-}
-
-template <bool P64>
-__device__ __forceinline__ void rotate(const SampleRot& r, const typename ParamTraits<P64>::Beam& e,
-                                       double& vx, double& vy, double& vz) {
-  if constexpr (P64)
-    rot_f64(r, e.x, e.y, e.z, vx, vy, vz);
-  else
-    rot_ref32(r, e.x, e.y, e.z, vx, vy, vz);
 }
 
 template <typename MapT>
@@ -199,153 +174,450 @@ __device__ __forceinline__ double warp_sum(double v) {
   return v;
 }
 
-// One pass of a warp over beam pixels [s_begin, s_end) of a chunk held in
-// shared memory, accumulating into acc[0..3].
-template <int MODE, bool HAS_QU, typename MapT, bool P64>
-__device__ __forceinline__ void accumulate_chunk(const KArgs& a, const SampleRot& rot, double z_pts,
-                                                 double sth_pts, double phi_pts,
-                                                 const typename ParamTraits<P64>::Beam* sm, int n,
-                                                 double acc[4], unsigned long long& nerr) {
-  const int lane = threadIdx.x & 31;
-  for (int i = lane; i < n; i += 32) {
-    const typename ParamTraits<P64>::Beam e = sm[i];
-    double vx, vy, vz;
-    rotate<P64>(rot, e, vx, vy, vz);
-    const float bvf = e.w;
-    const double bv = (double)bvf;
-    double phi_w = atan2(vy, vx);
-    if (phi_w < 0.0) phi_w += kTwoPi;
-    if constexpr (MODE == TODGPU_BILINEAR) {
-      const double z = clamp1(vz);
-      Stencil st;
-      hp_stencil(a.nside, z, phi_w, a.npix, st);
-      bool ok = true;
-#pragma unroll
-      for (int k = 0; k < 4; ++k) ok = ok && ((unsigned long long)st.p[k] < (unsigned long long)a.npix);
-      if (!ok) {
-        ++nerr;
-        continue;
+// ---------------------------------------------------------------------------
+// Ring table (global memory, built once per nside and footprint reach) and
+// the per-sample spin-2 table (shared memory).
+// ---------------------------------------------------------------------------
+
+// One RING ring.  Record 0 is a header: z = nside, ta = reach [rad].
+struct __align__(16) RingRec {
+  double z;      // ring centre z
+  double ta;     // acos(z)
+  double sth;    // sqrt(max(0, 1 - z^2))
+  double phi0;   // longitude of the first pixel
+  double dphi;   // pixel spacing
+  long long first;
+  int n;         // pixels in the ring
+  int cap;       // spin-2 table slots reserved for this ring
+  long long pre; // sum of cap over rings 1 .. ir-1
+};
+static_assert(sizeof(RingRec) == 64, "RingRec must be 64 bytes");
+
+// Ring provider backed by the global ring table.
+struct TableRings {
+  const RingRec* t;
+  __device__ __forceinline__ RingData operator()(long long ir) const {
+    const RingRec* r = t + ir;
+    RingData d;
+    d.z = __ldg(&r->z);
+    d.ta = __ldg(&r->ta);
+    d.phi0 = __ldg(&r->phi0);
+    d.dphi = __ldg(&r->dphi);
+    d.first = __ldg(&r->first);
+    d.n = __ldg(&r->n);
+    return d;
+  }
+  __device__ __forceinline__ double sth(long long ir, const RingData&) const { return __ldg(&t[ir].sth); }
+};
+
+// Per-sample spin-2 table: for window ring r (ring ir_lo + r) the slots
+// [off[r], off[r] + cap_r) hold cos 2d / sin 2d of in-ring pixels
+// iplo[r], iplo[r] + 1, ... (mod n).
+struct Spin2Tab {
+  long long ir_lo;
+  int nr;        // window rings (0: no table for this sample)
+  int total;     // filled slots
+  int off[kRingCap];
+  int iplo[kRingCap];
+  int cap[kRingCap];
+};
+
+struct Bore {
+  double z, sth, phi;
+};
+
+__device__ __forceinline__ void spin2_lookup(const Spin2Tab& w, const double2* tab, long long ring, long long ip,
+                                             long long n, double zn, double phin, const Bore& bo, double& c2d,
+                                             double& s2d) {
+  // ip is the pixel's in-ring index and n its ring's length; the spill case
+  // (ip == n) and anything outside the window use direct evaluation.
+  const long long r = ring - w.ir_lo;
+  if ((unsigned long long)r < (unsigned long long)w.nr && (unsigned long long)ip < (unsigned long long)n) {
+    long long j = ip - w.iplo[r];
+    if (j < 0) j += n;
+    if (j >= 0 && j < w.cap[r]) {
+      const long long slot = w.off[r] + j;
+      if (slot < w.total) {
+        const double2 v = tab[slot];
+        c2d = v.x;
+        s2d = v.y;
+        return;
       }
-      if constexpr (HAS_QU) {
-        double c2[4], s2[4], q[4], u[4];
+    }
+  }
+  const double sth_n = sqrt(max0(1.0 - zn * zn));
+  spin2_c2s2(zn, sth_n, phin, bo.z, bo.sth, bo.phi, c2d, s2d);
+}
+
+// Beam centre direction (normalised mean of the beam vectors) and the
+// largest angle between it and any beam vector; block-wide, once per CTA.
+template <bool P64, int NT>
+__device__ void beam_extent(const KArgs& a, double* s_red, double& cx, double& cy, double& cz, double& radius) {
+  constexpr int NW = NT / 32;
+  double sx = 0.0, sy = 0.0, sz = 0.0;
+  for (long long s = threadIdx.x; s < a.S; s += NT) {
+    if constexpr (P64) {
+      const double* v = static_cast<const double*>(a.vec) + 3 * s;
+      sx += v[0];
+      sy += v[1];
+      sz += v[2];
+    } else {
+      const float* v = static_cast<const float*>(a.vec) + 3 * s;
+      sx += (double)v[0];
+      sy += (double)v[1];
+      sz += (double)v[2];
+    }
+  }
+  sx = warp_sum(sx);
+  sy = warp_sum(sy);
+  sz = warp_sum(sz);
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  if (lane == 0) {
+    s_red[warp * 4 + 0] = sx;
+    s_red[warp * 4 + 1] = sy;
+    s_red[warp * 4 + 2] = sz;
+  }
+  __syncthreads();
+  sx = sy = sz = 0.0;
+  for (int i = 0; i < NW; ++i) {
+    sx += s_red[i * 4 + 0];
+    sy += s_red[i * 4 + 1];
+    sz += s_red[i * 4 + 2];
+  }
+  const double nrm = sqrt(sx * sx + sy * sy + sz * sz);
+  if (nrm > 0.0) {
+    cx = sx / nrm;
+    cy = sy / nrm;
+    cz = sz / nrm;
+  } else {
+    cx = 0.0;
+    cy = 0.0;
+    cz = 1.0;
+  }
+  double mind = 1.0;
+  for (long long s = threadIdx.x; s < a.S; s += NT) {
+    double vx, vy, vz;
+    if constexpr (P64) {
+      const double* v = static_cast<const double*>(a.vec) + 3 * s;
+      vx = v[0];
+      vy = v[1];
+      vz = v[2];
+    } else {
+      const float* v = static_cast<const float*>(a.vec) + 3 * s;
+      vx = v[0];
+      vy = v[1];
+      vz = v[2];
+    }
+    const double vn = sqrt(vx * vx + vy * vy + vz * vz);
+    const double d = vn > 0.0 ? (vx * cx + vy * cy + vz * cz) / vn : -1.0;
+    mind = fmin(mind, d);
+  }
 #pragma unroll
-        for (int k = 0; k < 4; ++k) {
-          const double sth_n = sqrt(max0(1.0 - st.zn[k] * st.zn[k]));
-          spin2_c2s2(st.zn[k], sth_n, st.phin[k], z_pts, sth_pts, phi_pts, c2[k], s2[k]);
-          q[k] = map_at<MapT>(a, a.c_q, st.p[k]);
-          u[k] = map_at<MapT>(a, a.c_u, st.p[k]);
-        }
-        double tq = (st.w[0] * (q[0] * c2[0] + u[0] * s2[0]) + st.w[1] * (q[1] * c2[1] + u[1] * s2[1]) +
-                     st.w[2] * (q[2] * c2[2] + u[2] * s2[2]) + st.w[3] * (q[3] * c2[3] + u[3] * s2[3])) *
-                    bv;
-        double tu = (st.w[0] * (-q[0] * s2[0] + u[0] * c2[0]) + st.w[1] * (-q[1] * s2[1] + u[1] * c2[1]) +
-                     st.w[2] * (-q[2] * s2[2] + u[2] * c2[2]) + st.w[3] * (-q[3] * s2[3] + u[3] * c2[3])) *
-                    bv;
+  for (int o = 16; o > 0; o >>= 1) mind = fmin(mind, __shfl_xor_sync(0xffffffffu, mind, o));
+  __syncthreads();
+  if (lane == 0) s_red[warp] = mind;
+  __syncthreads();
+  mind = 1.0;
+  for (int i = 0; i < NW; ++i) mind = fmin(mind, s_red[i]);
+  __syncthreads();
+  radius = acos(clamp1(mind));
+}
+
+// One beam pixel's contribution, accumulated into acc[0..3].
+template <int MODE, bool HAS_QU, typename MapT, bool P64, class Rings>
+__device__ __forceinline__ void eval_pixel(const KArgs& a, const SampleRot& rot, const Bore& bo, const Rings& rings,
+                                           const Spin2Tab& w, const double2* tab, long long s, double acc[4],
+                                           unsigned long long& nerr) {
+  double vx, vy, vz;
+  rotate_pixel<P64>(a, rot, s, vx, vy, vz);
+  const float bvf = __ldg(a.beam + s);
+  const double bv = (double)bvf;
+  double phi_w = atan2(vy, vx);
+  if (phi_w < 0.0) phi_w += kTwoPi;
+  if constexpr (MODE == TODGPU_BILINEAR) {
+    const double z = clamp1(vz);
+    // Per-neighbour terms are summed in the reference's order k = 0..3.
+    double tq = 0.0, tu = 0.0, to[4] = {0.0, 0.0, 0.0, 0.0};
+    bool ok = true;
+    hp_stencil(a.nside, z, phi_w, rings,
+               [&](int k, long long p, double wk, long long ring, long long ip, long long n, double zn,
+                   double phin) {
+                 if ((unsigned long long)p >= (unsigned long long)a.npix) {
+                   ok = false;
+                   return;
+                 }
+                 if constexpr (HAS_QU) {
+                   double c2, s2;
+                   spin2_lookup(w, tab, ring, ip, n, zn, phin, bo, c2, s2);
+                   const double q = map_at<MapT>(a, a.c_q, p);
+                   const double u = map_at<MapT>(a, a.c_u, p);
+                   const double vq = wk * (q * c2 + u * s2);
+                   const double vu = wk * (-q * s2 + u * c2);
+                   tq = (k == 0) ? vq : tq + vq;
+                   tu = (k == 0) ? vu : tu + vu;
+                 }
 #pragma unroll
-        for (int c = 0; c < 4; ++c) {
-          if (c >= a.C) break;
-          if (c == a.c_q) {
-            acc[c] += tq;
-          } else if (c == a.c_u) {
-            acc[c] += tu;
-          } else {
-            acc[c] += (st.w[0] * map_at<MapT>(a, c, st.p[0]) + st.w[1] * map_at<MapT>(a, c, st.p[1]) +
-                       st.w[2] * map_at<MapT>(a, c, st.p[2]) + st.w[3] * map_at<MapT>(a, c, st.p[3])) *
-                      bv;
-          }
-        }
-      } else {
+                 for (int c = 0; c < 4; ++c) {
+                   if (c >= a.C) break;
+                   if (HAS_QU && (c == a.c_q || c == a.c_u)) continue;
+                   const double v = wk * map_at<MapT>(a, c, p);
+                   to[c] = (k == 0) ? v : to[c] + v;
+                 }
+               });
+    if (!ok) {
+      ++nerr;
+      return;
+    }
 #pragma unroll
-        for (int c = 0; c < 4; ++c) {
-          if (c >= a.C) break;
-          acc[c] += (st.w[0] * map_at<MapT>(a, c, st.p[0]) + st.w[1] * map_at<MapT>(a, c, st.p[1]) +
-                     st.w[2] * map_at<MapT>(a, c, st.p[2]) + st.w[3] * map_at<MapT>(a, c, st.p[3])) *
-                    bv;
-        }
+    for (int c = 0; c < 4; ++c) {
+      if (c >= a.C) break;
+      if (HAS_QU && c == a.c_q)
+        acc[c] += tq * bv;
+      else if (HAS_QU && c == a.c_u)
+        acc[c] += tu * bv;
+      else
+        acc[c] += to[c] * bv;
+    }
+  } else {
+    const double sin_th = sqrt(max0(vx * vx + vy * vy));
+    const Nearest nb = hp_nearest(a.nside, vz, sin_th, phi_w, rings);
+    if ((unsigned long long)nb.pix >= (unsigned long long)a.npix) {
+      ++nerr;
+      return;
+    }
+    if constexpr (HAS_QU) {
+      double c2d, s2d;
+      spin2_lookup(w, tab, nb.ring, nb.ip, nb.n, nb.zc, nb.phic, bo, c2d, s2d);
+      const double qv = map_at<MapT>(a, a.c_q, nb.pix);
+      const double uv = map_at<MapT>(a, a.c_u, nb.pix);
+#pragma unroll
+      for (int c = 0; c < 4; ++c) {
+        if (c >= a.C) break;
+        if (c == a.c_q)
+          acc[c] += (qv * c2d + uv * s2d) * bv;
+        else if (c == a.c_u)
+          acc[c] += (-qv * s2d + uv * c2d) * bv;
+        else
+          acc[c] += map_x_beam<MapT>(a, c, nb.pix, bvf);
       }
     } else {
-      const double sin_th = sqrt(max0(vx * vx + vy * vy));
-      const Nearest nb = hp_nearest(a.nside, vz, sin_th, phi_w, a.npix);
-      if ((unsigned long long)nb.pix >= (unsigned long long)a.npix) {
-        ++nerr;
-        continue;
-      }
-      if constexpr (HAS_QU) {
-        const double sth_n = sqrt(max0(1.0 - nb.zc * nb.zc));
-        double c2d, s2d;
-        spin2_c2s2(nb.zc, sth_n, nb.phic, z_pts, sth_pts, phi_pts, c2d, s2d);
-        const double qv = map_at<MapT>(a, a.c_q, nb.pix);
-        const double uv = map_at<MapT>(a, a.c_u, nb.pix);
 #pragma unroll
-        for (int c = 0; c < 4; ++c) {
-          if (c >= a.C) break;
-          if (c == a.c_q)
-            acc[c] += (qv * c2d + uv * s2d) * bv;
-          else if (c == a.c_u)
-            acc[c] += (-qv * s2d + uv * c2d) * bv;
-          else
-            acc[c] += map_x_beam<MapT>(a, c, nb.pix, bvf);
-        }
-      } else {
-#pragma unroll
-        for (int c = 0; c < 4; ++c) {
-          if (c >= a.C) break;
-          acc[c] += map_x_beam<MapT>(a, c, nb.pix, bvf);
-        }
+      for (int c = 0; c < 4; ++c) {
+        if (c >= a.C) break;
+        acc[c] += map_x_beam<MapT>(a, c, nb.pix, bvf);
       }
     }
   }
 }
 
-template <int MODE, bool HAS_QU, typename MapT, bool P64>
-__global__ void __launch_bounds__(kThreads) gather_accum_kernel(const KArgs a) {
-  using Beam = typename ParamTraits<P64>::Beam;
-  constexpr int kChunk = ParamTraits<P64>::kChunk;
-  extern __shared__ __align__(16) unsigned char smem_raw[];
-  Beam* sm = reinterpret_cast<Beam*>(smem_raw);
+// Flush the per-warp partial sums of sample `b` into tod (fixed order).
+template <int NW>
+__device__ __forceinline__ void flush_sample(const KArgs& a, const double* s_red, long long b) {
+#pragma unroll
+  for (int c = 0; c < 4; ++c) {
+    if (c >= a.C) break;
+    double v = 0.0;
+    for (int i = 0; i < NW; ++i) v += s_red[i * 4 + c];
+    a.tod[(long long)c * a.tod_stride + b] += v;
+  }
+}
 
-  const int warp = threadIdx.x >> 5;
-  const int lane = threadIdx.x & 31;
-  const long long n_chunks = (a.S + kChunk - 1) / kChunk;
-  const bool resident = (n_chunks == 1);
-  if (resident) {
-    stage_beam<P64>(a, sm, 0, (int)a.S);
-    __syncthreads();
+// Main kernel.  With a ring table: ring data come from it and, when the
+// entry carries Q and U, each sample's footprint gets a spin-2 table in
+// shared memory.  Without one: everything is evaluated directly.
+template <int MODE, bool HAS_QU, typename MapT, bool P64, int NT, int MINB>
+__global__ void __launch_bounds__(NT, MINB) gather_accum_kernel(const KArgs a) {
+  constexpr int NW = NT / 32;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  Spin2Tab& w = *reinterpret_cast<Spin2Tab*>(smem_raw);
+  double2* tab = reinterpret_cast<double2*>(smem_raw + ((sizeof(Spin2Tab) + 15) & ~size_t(15)));
+  __shared__ double s_red[NW * 4];
+
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const RingRec* rt = static_cast<const RingRec*>(a.ring_table);
+  double cx = 0.0, cy = 0.0, cz = 1.0, reach = 0.0;
+  bool use_tab = false;
+  if (rt != nullptr && HAS_QU) {
+    double rbeam;
+    beam_extent<P64, NT>(a, s_red, cx, cy, cz, rbeam);
+    // stencil neighbours lie within ~3 pixel sizes of the query: 4/nside
+    // rad, plus slack for the float32 parameter rounding
+    reach = rbeam + 4.0 / (double)a.nside + 1e-5;
+    use_tab = reach <= __ldg(&rt[0].ta);
+  }
+  if (threadIdx.x == 0) {
+    w.nr = 0;
+    w.total = 0;
   }
   unsigned long long nerr = 0;
-  for (long long tile = (long long)blockIdx.x * kWarps; tile < a.B; tile += (long long)gridDim.x * kWarps) {
-    const long long b = tile + warp;
-    const bool active = (b < a.B);
-    SampleRot rot;
-    double z_pts = 0.0, sth_pts = 0.0, phi_pts = 0.0;
-    if (active) {
-      rot = load_rot<P64>(a, b);
-      if (HAS_QU) load_boresight<P64>(a, b, z_pts, sth_pts, phi_pts);
+  long long prev = -1;
+  for (long long b = blockIdx.x; b < a.B; b += gridDim.x) {
+    const SampleRot rot = load_rot<P64>(a, b);
+    Bore bo{0.0, 0.0, 0.0};
+    if (HAS_QU) load_boresight<P64>(a, b, bo.z, bo.sth, bo.phi);
+    __syncthreads();  // previous sample is done with the table and its partial sums
+    if (prev >= 0 && threadIdx.x == 0) flush_sample<NW>(a, s_red, prev);
+    if (use_tab) {
+      // footprint window of this sample (same values in every thread)
+      double ux, uy, uz;
+      rot_f64(rot, cx, cy, cz, ux, uy, uz);
+      const double theta_u = acos(clamp1(uz));
+      double phi_u = atan2(uy, ux);
+      if (phi_u < 0.0) phi_u += kTwoPi;
+      const double th_lo = theta_u - reach, th_hi = theta_u + reach;
+      long long ir_lo = th_lo <= 0.0 ? 1 : hp_ring_above(a.nside, cos(th_lo));
+      long long ir_hi = th_hi >= kPi ? 4 * a.nside - 1 : hp_ring_above(a.nside, cos(th_hi)) + 1;
+      ir_lo = max(ir_lo, 1LL);
+      ir_hi = min(ir_hi, 4 * a.nside - 1);
+      // a non-finite footprint centre gives an empty or invalid window: no table
+      const long long nr = ir_hi - ir_lo + 1;
+      bool fits = nr > 0 && nr <= kRingCap && ir_lo >= 1 && ir_hi <= 4 * a.nside - 1;
+      long long base = 0, total = 0;
+      if (fits) {
+        base = __ldg(&rt[ir_lo].pre);
+        total = __ldg(&rt[ir_hi].pre) + __ldg(&rt[ir_hi].cap) - base;
+        fits = total <= a.tab_cap;
+      }
+      if (fits) {
+        for (int t = threadIdx.x; t < nr; t += NT) {
+          const RingRec* r = rt + ir_lo + t;
+          const int n = __ldg(&r->n), cap = __ldg(&r->cap);
+          int iplo = 0;
+          if (cap < n) {
+            const double c = floor((phi_u - __ldg(&r->phi0)) / __ldg(&r->dphi));
+            iplo = (int)py_imod((long long)c - (cap - 1) / 2, n);
+          }
+          w.off[t] = (int)(__ldg(&r->pre) - base);
+          w.iplo[t] = iplo;
+          w.cap[t] = cap;
+        }
+      }
+      if (threadIdx.x == 0) {
+        w.ir_lo = ir_lo;
+        w.nr = fits ? (int)nr : 0;
+        w.total = fits ? (int)total : 0;
+      }
+      __syncthreads();
+      const int ntab = w.total, nwin = w.nr;
+      for (int e = threadIdx.x; e < ntab; e += NT) {
+        int lo = 0, hi = nwin - 1;  // last window ring with off <= e
+        while (lo < hi) {
+          const int mid = (lo + hi + 1) >> 1;
+          if (w.off[mid] <= e)
+            lo = mid;
+          else
+            hi = mid - 1;
+        }
+        const RingRec* r = rt + w.ir_lo + lo;
+        const int n = __ldg(&r->n);
+        int ip = w.iplo[lo] + (e - w.off[lo]);
+        if (ip >= n) ip -= n;
+        const double phin = __ldg(&r->phi0) + (double)ip * __ldg(&r->dphi);
+        double c2, s2;
+        spin2_c2s2(__ldg(&r->z), __ldg(&r->sth), phin, bo.z, bo.sth, bo.phi, c2, s2);
+        tab[e] = make_double2(c2, s2);
+      }
     }
+    __syncthreads();
+
     double acc[4] = {0.0, 0.0, 0.0, 0.0};
-    for (long long ch = 0; ch < n_chunks; ++ch) {
-      const long long s0 = ch * kChunk;
-      const int n = (int)min((long long)kChunk, a.S - s0);
-      if (!resident) {
-        __syncthreads();
-        stage_beam<P64>(a, sm, s0, n);
-        __syncthreads();
-      }
-      if (active) accumulate_chunk<MODE, HAS_QU, MapT, P64>(a, rot, z_pts, sth_pts, phi_pts, sm, n, acc, nerr);
+    if (rt != nullptr) {
+      const TableRings rings{rt};
+      for (long long s = threadIdx.x; s < a.S; s += NT)
+        eval_pixel<MODE, HAS_QU, MapT, P64>(a, rot, bo, rings, w, tab, s, acc, nerr);
+    } else {
+      const DirectRings rings{a.nside, a.npix};
+      for (long long s = threadIdx.x; s < a.S; s += NT)
+        eval_pixel<MODE, HAS_QU, MapT, P64>(a, rot, bo, rings, w, tab, s, acc, nerr);
     }
-    if (active) {
 #pragma unroll
-      for (int c = 0; c < 4; ++c) {
-        if (c >= a.C) break;
-        const double v = warp_sum(acc[c]);
-        if (lane == 0) a.tod[(long long)c * a.tod_stride + b] += v;
-      }
+    for (int c = 0; c < 4; ++c) {
+      if (c >= a.C) break;
+      const double v = warp_sum(acc[c]);
+      if (lane == 0) s_red[warp * 4 + c] = v;
     }
+    prev = b;
   }
+  __syncthreads();
+  if (prev >= 0 && threadIdx.x == 0) flush_sample<NW>(a, s_red, prev);
   if (a.err != nullptr) {
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) nerr += __shfl_xor_sync(0xffffffffu, nerr, o);
     if (lane == 0 && nerr) atomicAdd(a.err, nerr);
+  }
+}
+
+// Ring table: record ir (1 .. 4 nside - 1) of every ring; record 0 holds
+// nside and the reach.  cap_r bounds the pixels of ring r inside any disc of
+// radius `reach`: a disc meets the latitude of the ring in a longitude
+// interval of half-width at most asin(sin(reach) / sin(theta_r)), or the
+// whole ring when the disc can contain the pole.
+__global__ void ring_table_kernel(long long nside, double reach, RingRec* t) {
+  const long long nrings = 4 * nside - 1;
+  const long long npix = 12 * nside * nside;
+  for (long long ir = 1 + blockIdx.x * (long long)blockDim.x + threadIdx.x; ir <= nrings;
+       ir += (long long)gridDim.x * blockDim.x) {
+    const RingInfo ri = hp_ring_info(nside, ir, npix);
+    RingRec r;
+    r.z = hp_ring_z(nside, ir);
+    r.ta = acos(r.z);
+    r.sth = sqrt(max0(1.0 - r.z * r.z));
+    r.phi0 = ri.phi0;
+    r.dphi = ri.dphi;
+    r.first = ri.first;
+    r.n = (int)ri.n;
+    int cap = (int)ri.n;
+    if (reach < r.ta && reach < kPi - r.ta) {
+      const double x = sin(reach) / r.sth;
+      if (x < 1.0) {
+        const double half = asin(x);
+        const long long c = 2 * (long long)ceil(half / ri.dphi) + 5;
+        cap = (int)min(c, ri.n);
+      }
+    }
+    r.cap = cap;
+    r.pre = 0;
+    t[ir] = r;
+  }
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    RingRec h;
+    h.z = (double)nside;
+    h.ta = reach;
+    h.sth = 0.0;
+    h.phi0 = 0.0;
+    h.dphi = 0.0;
+    h.first = 0;
+    h.n = 0;
+    h.cap = 0;
+    h.pre = 0;
+    t[0] = h;
+  }
+}
+
+// Exclusive prefix sum of cap over rings 1..nrings into `pre` (one CTA of
+// 1024 threads: per-thread chunk sums, a block scan, then the chunks).
+__global__ void ring_prefix_kernel(long long nside, RingRec* t) {
+  __shared__ long long part[1024];
+  const long long nrings = 4 * nside - 1;
+  const long long chunk = (nrings + blockDim.x - 1) / blockDim.x;
+  const long long lo = 1 + threadIdx.x * chunk, hi = min(nrings + 1, lo + chunk);
+  long long sum = 0;
+  for (long long ir = lo; ir < hi; ++ir) sum += t[ir].cap;
+  part[threadIdx.x] = sum;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    long long run = 0;
+    for (int i = 0; i < (int)blockDim.x; ++i) {
+      const long long v = part[i];
+      part[i] = run;
+      run += v;
+    }
+  }
+  __syncthreads();
+  long long run = part[threadIdx.x];
+  for (long long ir = lo; ir < hi; ++ir) {
+    t[ir].pre = run;
+    run += t[ir].cap;
   }
 }
 
@@ -371,13 +643,11 @@ __global__ void stencil_kernel(const KArgs a, long long* pix, double* wgt) {
     const double z = clamp1(vz);
     double phi_w = atan2(vy, vx);
     if (phi_w < 0.0) phi_w += kTwoPi;
-    Stencil st;
-    hp_stencil(a.nside, z, phi_w, a.npix, st);
-#pragma unroll
-    for (int k = 0; k < 4; ++k) {
-      pix[k * BS + n] = st.p[k];
-      wgt[k * BS + n] = st.w[k];
-    }
+    hp_stencil(a.nside, z, phi_w, DirectRings{a.nside, a.npix},
+               [&](int k, long long p, double wk, long long, long long, long long, double, double) {
+                 pix[k * BS + n] = p;
+                 wgt[k * BS + n] = wk;
+               });
   }
 }
 
@@ -468,7 +738,7 @@ __global__ void ang2pix_kernel(long long nside, const double* theta, const doubl
     } else {
       phi_w = 0.0;
     }
-    out[i] = hp_nearest(nside, z, sin(theta[i]), phi_w, npix).pix;
+    out[i] = hp_nearest(nside, z, sin(theta[i]), phi_w, DirectRingsNoAcos{nside, npix}).pix;
   }
 }
 
@@ -527,31 +797,40 @@ struct LaunchInfo {
   bool configured = false;
 };
 
+constexpr size_t kTabHeaderBytes = (sizeof(Spin2Tab) + 15) & ~size_t(15);
+#ifndef TODGPU_CTA_THREADS
+#define TODGPU_CTA_THREADS 256
+#endif
+#ifndef TODGPU_CTA_MINB
+#define TODGPU_CTA_MINB 3
+#endif
+constexpr int kNT = TODGPU_CTA_THREADS;  // threads per CTA
+constexpr int kMinB = TODGPU_CTA_MINB;   // CTAs per SM the register budget is sized for
+
 template <int MODE, bool HAS_QU, typename MapT, bool P64>
-static int launch_gather(const KArgs& k, cudaStream_t stream) {
-  using Beam = typename ParamTraits<P64>::Beam;
-  constexpr int kChunk = ParamTraits<P64>::kChunk;
-  auto kern = gather_accum_kernel<MODE, HAS_QU, MapT, P64>;
+static int launch_gather(KArgs k, cudaStream_t stream) {
+  auto kern = gather_accum_kernel<MODE, HAS_QU, MapT, P64, kNT, kMinB>;
   static LaunchInfo info;
   static std::mutex mu;
-  const size_t smem_max = sizeof(Beam) * kChunk;
+  const int tab_cap = (HAS_QU && k.ring_table != nullptr) ? kTabCapDefault : 0;
+  const size_t smem = kTabHeaderBytes + sizeof(double2) * (size_t)tab_cap;
+  const size_t smem_max = kTabHeaderBytes + sizeof(double2) * (size_t)kTabCapDefault;
   {
     std::lock_guard<std::mutex> lock(mu);
     if (!info.configured) {
       cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_max);
       if (e != cudaSuccess) return cuda_fail(e, "cudaFuncSetAttribute");
       int nb = 0;
-      e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, kern, kThreads, smem_max);
+      e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, kern, kNT, smem_max);
       if (e != cudaSuccess) return cuda_fail(e, "cudaOccupancyMaxActiveBlocksPerMultiprocessor");
       info.blocks_per_sm = std::max(nb, 1);
       info.configured = true;
     }
   }
-  const long long tiles = (k.B + kWarps - 1) / kWarps;
+  k.tab_cap = tab_cap;
   const long long max_blocks = (long long)sm_count() * info.blocks_per_sm;
-  const int grid = (int)std::max(1LL, std::min(tiles, max_blocks));
-  const size_t smem = sizeof(Beam) * (size_t)std::min<long long>(k.S, kChunk);
-  kern<<<grid, kThreads, smem, stream>>>(k);
+  const int grid = (int)std::max(1LL, std::min(k.B, max_blocks));
+  kern<<<grid, kNT, smem, stream>>>(k);
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return cuda_fail(e, "gather_accum_kernel launch");
   return TODGPU_OK;
@@ -627,6 +906,9 @@ static KArgs make_kargs(const todgpu_gather_args* a) {
   k.tod = a->tod;
   k.tod_stride = a->tod_stride;
   k.err = a->err_count;
+  k.ring_table = (a->flags & TODGPU_FLAG_NO_TABLES) ? nullptr : a->ring_table;
+  if (k.ring_table != nullptr && (((uintptr_t)k.ring_table & 15) != 0)) k.ring_table = nullptr;
+  k.tab_cap = 0;
   return k;
 }
 
@@ -737,6 +1019,25 @@ extern "C" int todgpu_boresight_phi_host(const float* ax_pts, int64_t B, float* 
   }
   for (auto& th : pool) th.join();
   return TODGPU_OK;
+}
+
+extern "C" size_t todgpu_ring_table_bytes(int64_t nside) {
+  if (nside < 1 || nside > kMaxNside) return 0;
+  return sizeof(RingRec) * (size_t)(4 * nside);
+}
+
+extern "C" int todgpu_ring_table_build(int64_t nside, double reach, void* table, size_t bytes, void* stream) {
+  if (nside < 1 || nside > kMaxNside) return fail(TODGPU_ENSIDE, "nside out of range");
+  if (!table) return fail(TODGPU_EINVAL, "NULL table");
+  if (bytes < todgpu_ring_table_bytes(nside)) return fail(TODGPU_ESHAPE, "ring table buffer too small");
+  if (((uintptr_t)table & 15) != 0) return fail(TODGPU_EINVAL, "ring table must be 16-byte aligned");
+  if (!(reach >= 0.0) || !(reach <= kPi)) return fail(TODGPU_EINVAL, "reach must be in [0, pi]");
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  RingRec* t = static_cast<RingRec*>(table);
+  ring_table_kernel<<<grid_for(4 * nside, 256), 256, 0, s>>>(nside, reach, t);
+  ring_prefix_kernel<<<1, 1024, 0, s>>>(nside, t);
+  cudaError_t e = cudaGetLastError();
+  return e == cudaSuccess ? TODGPU_OK : cuda_fail(e, "ring table kernels");
 }
 
 extern "C" int todgpu_abi_version(void) { return TODGPU_ABI_VERSION; }

@@ -57,8 +57,48 @@ def boresight_phi_host(ax_pts) -> np.ndarray:
     return out
 
 
+_RING_TABLES = {}
+_REACH_STEP = 1e-4  # ring tables are built for reaches rounded up to this step [rad]
+
+
+def beam_reach(vec_orig, nside):
+    """Angular radius [rad] that every stencil neighbour of the rotated beam
+    stays within around the rotated beam centre: the beam's radius about its
+    mean direction plus 4/nside (stencil reach) plus float32 slack."""
+    v = vec_orig.detach().cpu().numpy() if is_tensor(vec_orig) else np.asarray(vec_orig)
+    v = np.asarray(v, np.float64).reshape(-1, 3)
+    if v.shape[0] == 0:
+        return 0.0
+    c = v.sum(axis=0)
+    nc = np.linalg.norm(c)
+    c = c / nc if nc > 0 else np.array([0.0, 0.0, 1.0])
+    vn = np.linalg.norm(v, axis=1)
+    with np.errstate(invalid="ignore", divide="ignore"):
+        d = np.where(vn > 0, (v @ c) / vn, -1.0)
+    r = float(np.arccos(np.clip(d.min(), -1.0, 1.0)))
+    return r + 4.0 / float(nside) + 2e-5
+
+
+def ring_table(nside, reach, device=None):
+    """Device ring table for ``nside`` covering footprints up to ``reach``
+    (built once and cached per device, nside and rounded reach)."""
+    dev = device if device is not None else require_cuda()
+    reach_q = min(np.pi, np.ceil(reach / _REACH_STEP) * _REACH_STEP)
+    key = (dev.index if isinstance(dev, torch.device) else int(dev), int(nside), round(reach_q / _REACH_STEP))
+    t = _RING_TABLES.get(key)
+    if t is None:
+        nbytes = int(_native.lib().todgpu_ring_table_bytes(int(nside)))
+        if nbytes == 0:
+            raise _native.TodGpuError(_native.ENSIDE, f"nside {nside} out of range")
+        t = torch.empty(nbytes // 8, dtype=torch.float64, device=dev)
+        _native.check(_native.lib().todgpu_ring_table_build(int(nside), float(reach_q), t.data_ptr(),
+                                                            nbytes, stream_handle()))
+        _RING_TABLES[key] = t
+    return t
+
+
 def make_args(interp, nside, B, S, C, c_q, c_u, params, pdt, bore_phi, beam, mp, tod,
-              err=None):
+              err=None, flags=0, table=None):
     a = _native.GatherArgs()
     a.abi_version = _native.ABI_VERSION
     a.interp = interp
@@ -78,6 +118,8 @@ def make_args(interp, nside, B, S, C, c_q, c_u, params, pdt, bore_phi, beam, mp,
     a.tod = ptr(tod)
     a.tod_stride = tod.stride(0)
     a.err_count = ptr(err)
+    a.flags = int(flags)
+    a.ring_table = ptr(table)
     return a
 
 
@@ -92,8 +134,15 @@ def _map_tensor(mp_stacked):
 
 
 def gather_accum(interp, vec_orig, axes, cos_a, sin_a, ax_pts, cos_p, sin_p, nside, mp_stacked,
-                 beam_vals, B, S, tod, c_q=-1, c_u=-1, bore_phi=None, err_count=None):
-    """One fused launch; see the module docstring.  Returns ``tod``."""
+                 beam_vals, B, S, tod, c_q=-1, c_u=-1, bore_phi=None, err_count=None, flags=0):
+    """One fused launch; see the module docstring.  Returns ``tod``.
+
+    ``err_count``: optional int64 CUDA tensor of one element that receives the
+    number of (sample, beam pixel) terms skipped because a stencil pixel fell
+    outside the map (only possible for non-finite pointing).
+    ``flags``: ``_native.FLAG_NO_TABLES`` evaluates every ring quantity and
+    spin-2 angle directly instead of from the per-sample footprint tables
+    (identical results; for testing)."""
     require_cuda()
     B = int(B)
     S = int(S)
@@ -125,8 +174,11 @@ def gather_accum(interp, vec_orig, axes, cos_a, sin_a, ax_pts, cos_p, sin_p, nsi
     if tuple(dtod.shape) != (C, B):
         raise ValueError(f"tod has shape {tuple(dtod.shape)}, expected {(C, B)}")
 
+    table = None
+    if not flags & _native.FLAG_NO_TABLES and B > 0 and S > 0:
+        table = ring_table(nside, beam_reach(vec_orig, nside), params[0].device)
     args = make_args(interp, nside, B, S, C, c_q, c_u, params, pdt, bphi, beam, mp, dtod,
-                     err_count)
+                     err_count, flags, table)
     _native.check(_native.lib().todgpu_gather_accum(ctypes.byref(args), stream_handle()))
     if host_tod is not None:
         res = dtod.cpu().numpy()

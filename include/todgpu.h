@@ -147,6 +147,13 @@ int todgpu_boresight_phi_host(const float *ax_pts, int64_t B, float *out, int32_
 size_t todgpu_ring_table_bytes(int64_t nside);
 int todgpu_ring_table_build(int64_t nside, double reach, void *table, size_t bytes, void *stream);
 
+/* FP64 pipe throughput probe (measurement helper; no counterpart in the
+ * reference): launches `blocks` CTAs of 256 threads running `iters` rounds of
+ * 8 independent FMA chains; *flops receives the floating-point operation count
+ * of the launch (host).  `sink` is a device buffer of `blocks` doubles that is
+ * never written in practice.  Time it with CUDA events on `stream`. */
+int todgpu_fp64_probe(int64_t blocks, int32_t iters, double *sink, double *flops, void *stream);
+
 /* Library introspection. */
 int todgpu_abi_version(void);
 const char *todgpu_last_error_string(void);

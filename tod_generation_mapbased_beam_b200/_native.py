@@ -91,6 +91,8 @@ def _declare(lib):
     lib.todgpu_ring_table_bytes.restype = ctypes.c_size_t
     lib.todgpu_ring_table_build.argtypes = [_i64, ctypes.c_double, _p, ctypes.c_size_t, _p]
     lib.todgpu_ring_table_build.restype = ctypes.c_int
+    lib.todgpu_fp64_probe.argtypes = [_i64, _i32, _p, ctypes.POINTER(ctypes.c_double), _p]
+    lib.todgpu_fp64_probe.restype = ctypes.c_int
     lib.todgpu_abi_version.argtypes = []
     lib.todgpu_abi_version.restype = ctypes.c_int
     lib.todgpu_last_error_string.argtypes = []
@@ -136,6 +138,7 @@ def exported_symbols():
         "todgpu_boresight_phi_host",
         "todgpu_ring_table_bytes",
         "todgpu_ring_table_build",
+        "todgpu_fp64_probe",
         "todgpu_abi_version",
         "todgpu_last_error_string",
     ]

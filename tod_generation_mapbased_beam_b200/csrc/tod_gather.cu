@@ -215,6 +215,7 @@ struct TableRings {
 // iplo[r], iplo[r] + 1, ... (mod n).
 struct Spin2Tab {
   long long ir_lo;
+  int ir_lo32;   // ir_lo as a 32-bit index (fast path)
   int nr;        // window rings (0: no table for this sample)
   int total;     // filled slots
   int off[kRingCap];
@@ -323,17 +324,14 @@ __device__ void beam_extent(const KArgs& a, double* s_red, double& cx, double& c
   radius = acos(clamp1(mind));
 }
 
-// One beam pixel's contribution, accumulated into acc[0..3].
+// One beam pixel's contribution, accumulated into acc[0..3]: generic path
+// (64-bit indices, any ring provider, any component layout).  Used without a
+// ring table and for non-finite rotated vectors.
 template <int MODE, bool HAS_QU, typename MapT, bool P64, class Rings>
-__device__ __forceinline__ void eval_pixel(const KArgs& a, const SampleRot& rot, const Bore& bo, const Rings& rings,
-                                           const Spin2Tab& w, const double2* tab, long long s, double acc[4],
-                                           unsigned long long& nerr) {
-  double vx, vy, vz;
-  rotate_pixel<P64>(a, rot, s, vx, vy, vz);
-  const float bvf = __ldg(a.beam + s);
+__device__ __noinline__ void eval_generic(const KArgs& a, const Bore& bo, const Rings& rings, const Spin2Tab& w,
+                                          const double2* tab, double vx, double vy, double vz, double phi_w,
+                                          float bvf, double acc[4], unsigned long long& nerr) {
   const double bv = (double)bvf;
-  double phi_w = atan2(vy, vx);
-  if (phi_w < 0.0) phi_w += kTwoPi;
   if constexpr (MODE == TODGPU_BILINEAR) {
     const double z = clamp1(vz);
     // Per-neighbour terms are summed in the reference's order k = 0..3.
@@ -356,9 +354,7 @@ __device__ __forceinline__ void eval_pixel(const KArgs& a, const SampleRot& rot,
                    tq = (k == 0) ? vq : tq + vq;
                    tu = (k == 0) ? vu : tu + vu;
                  }
-#pragma unroll
-                 for (int c = 0; c < 4; ++c) {
-                   if (c >= a.C) break;
+                 for (int c = 0; c < a.C; ++c) {
                    if (HAS_QU && (c == a.c_q || c == a.c_u)) continue;
                    const double v = wk * map_at<MapT>(a, c, p);
                    to[c] = (k == 0) ? v : to[c] + v;
@@ -368,9 +364,7 @@ __device__ __forceinline__ void eval_pixel(const KArgs& a, const SampleRot& rot,
       ++nerr;
       return;
     }
-#pragma unroll
-    for (int c = 0; c < 4; ++c) {
-      if (c >= a.C) break;
+    for (int c = 0; c < a.C; ++c) {
       if (HAS_QU && c == a.c_q)
         acc[c] += tq * bv;
       else if (HAS_QU && c == a.c_u)
@@ -390,9 +384,7 @@ __device__ __forceinline__ void eval_pixel(const KArgs& a, const SampleRot& rot,
       spin2_lookup(w, tab, nb.ring, nb.ip, nb.n, nb.zc, nb.phic, bo, c2d, s2d);
       const double qv = map_at<MapT>(a, a.c_q, nb.pix);
       const double uv = map_at<MapT>(a, a.c_u, nb.pix);
-#pragma unroll
-      for (int c = 0; c < 4; ++c) {
-        if (c >= a.C) break;
+      for (int c = 0; c < a.C; ++c) {
         if (c == a.c_q)
           acc[c] += (qv * c2d + uv * s2d) * bv;
         else if (c == a.c_u)
@@ -401,10 +393,250 @@ __device__ __forceinline__ void eval_pixel(const KArgs& a, const SampleRot& rot,
           acc[c] += map_x_beam<MapT>(a, c, nb.pix, bvf);
       }
     } else {
+      for (int c = 0; c < a.C; ++c) acc[c] += map_x_beam<MapT>(a, c, nb.pix, bvf);
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Fast path: finite rotated vector, ring table present, nside <= 8192 (all
+// ring and pixel indices fit 32 bits).  Same decisions and the same floating
+// point operations as the generic path, with 32-bit index arithmetic, ring
+// data from the table and a compile-time component layout.
+// ---------------------------------------------------------------------------
+
+constexpr int kLayoutGeneric = 0;  // runtime C, c_q, c_u
+constexpr int kLayoutIQU = 1;      // C = 3, Q at 1, U at 2
+
+struct RingFast {
+  int n, first;
+  double phi0, dphi, z, ta;
+};
+
+__device__ __forceinline__ RingFast ring_fast(const RingRec* rt, int ir) {
+  const RingRec* r = rt + ir;
+  RingFast d;
+  d.n = __ldg(&r->n);
+  d.first = (int)__ldg(&r->first);
+  d.phi0 = __ldg(&r->phi0);
+  d.dphi = __ldg(&r->dphi);
+  d.z = __ldg(&r->z);
+  d.ta = __ldg(&r->ta);
+  return d;
+}
+
+// hp_ring_above for a finite |z| <= 1 (int() of an in-range value truncates).
+__device__ __forceinline__ int ring_above_fast(int nside, double z) {
+  const double az = fabs(z);
+  if (az > kTwoThirds) {
+    const int ir = (int)((double)nside * sqrt(3.0 * (1.0 - az)));
+    return (z < 0.0) ? 4 * nside - ir - 1 : ir;
+  }
+  return (int)((double)nside * (2.0 - 1.5 * z));
+}
+
+// (x + d) mod n for 0 <= x <= n, 1 <= d <= 2 and n >= 4.
+__device__ __forceinline__ int wrap_up(int x, int d, int n) {
+  const int v = x + d;
+  return v >= n ? v - n : v;
+}
+
+// The bilinear stencil of hp_stencil with 32-bit indices; tw is in [0, n]
+// for finite phi in [0, 2 pi], so int(tw) is a plain truncation.
+template <class Visit>
+__device__ __forceinline__ void stencil_fast(int nside, double z, double phi_w, const RingRec* rt, Visit&& visit) {
+  const int ir_above = ring_above_fast(nside, z);
+  if (ir_above == 0) {
+    const RingFast ra = ring_fast(rt, 1);
+    const double tw = py_fmod_pos((phi_w - ra.phi0) / ra.dphi, (double)ra.n);
+    const int ip = (int)tw;
+    const double frac = tw - (double)ip;
+    const int ip2 = wrap_up(ip, 1, ra.n);
+    const int o1 = wrap_up(ip, 2, ra.n), o2 = wrap_up(ip2, 2, ra.n);
+    const double theta = acos(z);
+    const double wt = theta / ra.ta;
+    const double nf = (1.0 - wt) * 0.25;
+    visit(0, ra.first + o1, nf, 1, o1, ra.n, ra.z, ra.phi0 + (double)o1 * ra.dphi);
+    visit(1, ra.first + o2, nf, 1, o2, ra.n, ra.z, ra.phi0 + (double)o2 * ra.dphi);
+    visit(2, ra.first + ip, (1.0 - frac) * wt + nf, 1, ip, ra.n, ra.z, ra.phi0 + (double)ip * ra.dphi);
+    visit(3, ra.first + ip2, frac * wt + nf, 1, ip2, ra.n, ra.z, ra.phi0 + (double)ip2 * ra.dphi);
+  } else if (ir_above == 4 * nside - 1) {
+    const int ir_last = 4 * nside - 1;
+    const RingFast ra = ring_fast(rt, ir_last);
+    const double tw = py_fmod_pos((phi_w - ra.phi0) / ra.dphi, (double)ra.n);
+    const int ip = (int)tw;
+    const double frac = tw - (double)ip;
+    const int ip2 = wrap_up(ip, 1, ra.n);
+    const int o1 = wrap_up(ip, 2, ra.n), o2 = wrap_up(ip2, 2, ra.n);
+    const double theta = acos(z);
+    const double ws = (theta - ra.ta) / (kPi - ra.ta);
+    const double sf = ws * 0.25;
+    visit(0, ra.first + ip, (1.0 - frac) * (1.0 - ws) + sf, ir_last, ip, ra.n, ra.z, ra.phi0 + (double)ip * ra.dphi);
+    visit(1, ra.first + ip2, frac * (1.0 - ws) + sf, ir_last, ip2, ra.n, ra.z, ra.phi0 + (double)ip2 * ra.dphi);
+    visit(2, ra.first + o1, sf, ir_last, o1, ra.n, ra.z, ra.phi0 + (double)o1 * ra.dphi);
+    visit(3, ra.first + o2, sf, ir_last, o2, ra.n, ra.z, ra.phi0 + (double)o2 * ra.dphi);
+  } else {
+    const int ir_below = ir_above + 1;
+    const RingFast ra = ring_fast(rt, ir_above);
+    const RingFast rb = ring_fast(rt, ir_below);
+    const double theta = acos(z);
+    const double wb = (theta - ra.ta) / (rb.ta - ra.ta);
+    const double wa = 1.0 - wb;
+    double tw = py_fmod_pos((phi_w - ra.phi0) / ra.dphi, (double)ra.n);
+    const int ia = (int)tw;
+    const double fa = tw - (double)ia;
+    const int ia1 = wrap_up(ia, 1, ra.n);
+    visit(0, ra.first + ia, wa * (1.0 - fa), ir_above, ia, ra.n, ra.z, ra.phi0 + (double)ia * ra.dphi);
+    visit(1, ra.first + ia1, wa * fa, ir_above, ia1, ra.n, ra.z, ra.phi0 + (double)ia1 * ra.dphi);
+    tw = py_fmod_pos((phi_w - rb.phi0) / rb.dphi, (double)rb.n);
+    const int ib = (int)tw;
+    const double fb = tw - (double)ib;
+    const int ib1 = wrap_up(ib, 1, rb.n);
+    visit(2, rb.first + ib, wb * (1.0 - fb), ir_below, ib, rb.n, rb.z, rb.phi0 + (double)ib * rb.dphi);
+    visit(3, rb.first + ib1, wb * fb, ir_below, ib1, rb.n, rb.z, rb.phi0 + (double)ib1 * rb.dphi);
+  }
+}
+
+// Table lookup with 32-bit indices (ip == n is the spill case: direct).
+__device__ __forceinline__ void spin2_fast(const Spin2Tab& w, const double2* tab, int ring, int ip, int n, double zn,
+                                           double phin, const Bore& bo, double& c2d, double& s2d) {
+  const unsigned r = (unsigned)(ring - w.ir_lo32);
+  if (r < (unsigned)w.nr && (unsigned)ip < (unsigned)n) {
+    int j = ip - w.iplo[r];
+    j += (j >> 31) & n;
+    const int slot = w.off[r] + j;
+    if ((unsigned)j < (unsigned)w.cap[r] && slot < w.total) {
+      const double2 v = tab[slot];
+      c2d = v.x;
+      s2d = v.y;
+      return;
+    }
+  }
+  const double sth_n = sqrt(max0(1.0 - zn * zn));
+  spin2_c2s2(zn, sth_n, phin, bo.z, bo.sth, bo.phi, c2d, s2d);
+}
+
+template <int LAYOUT>
+struct Chan {
+  int C, q, u;
+  __device__ __forceinline__ explicit Chan(const KArgs& a) : C(a.C), q(a.c_q), u(a.c_u) {}
+};
+template <>
+struct Chan<kLayoutIQU> {
+  static constexpr int C = 3, q = 1, u = 2;
+  __device__ __forceinline__ explicit Chan(const KArgs&) {}
+};
+
+template <typename MapT>
+__device__ __forceinline__ double map_i(const KArgs& a, int c, int p) {
+  return (double)__ldg(static_cast<const MapT*>(a.map) + (long long)c * a.map_stride + p);
+}
+
+template <typename MapT>
+__device__ __forceinline__ double map_x_beam_i(const KArgs& a, int c, int p, float bv) {
+  const MapT m = __ldg(static_cast<const MapT*>(a.map) + (long long)c * a.map_stride + p);
+  if constexpr (sizeof(MapT) == 4)
+    return (double)(m * bv);
+  else
+    return m * (double)bv;
+}
+
+template <int MODE, bool HAS_QU, typename MapT, int LAYOUT>
+__device__ __forceinline__ void eval_fast(const KArgs& a, const Bore& bo, const RingRec* rt, const Spin2Tab& w,
+                                          const double2* tab, double vx, double vy, double vz, double phi_w,
+                                          float bvf, double acc[4]) {
+  const Chan<LAYOUT> ch(a);
+  const int nside = (int)a.nside;
+  const double bv = (double)bvf;
+  if constexpr (MODE == TODGPU_BILINEAR) {
+    const double z = clamp1(vz);
+    double tq = 0.0, tu = 0.0, to[4] = {0.0, 0.0, 0.0, 0.0};
+    stencil_fast(nside, z, phi_w, rt, [&](int k, int p, double wk, int ring, int ip, int n, double zn, double phin) {
+      if constexpr (HAS_QU) {
+        double c2, s2;
+        spin2_fast(w, tab, ring, ip, n, zn, phin, bo, c2, s2);
+        const double q = map_i<MapT>(a, ch.q, p);
+        const double u = map_i<MapT>(a, ch.u, p);
+        const double vq = wk * (q * c2 + u * s2);
+        const double vu = wk * (-q * s2 + u * c2);
+        tq = (k == 0) ? vq : tq + vq;
+        tu = (k == 0) ? vu : tu + vu;
+      }
 #pragma unroll
       for (int c = 0; c < 4; ++c) {
-        if (c >= a.C) break;
-        acc[c] += map_x_beam<MapT>(a, c, nb.pix, bvf);
+        if (c >= ch.C) break;
+        if (HAS_QU && (c == ch.q || c == ch.u)) continue;
+        const double v = wk * map_i<MapT>(a, c, p);
+        to[c] = (k == 0) ? v : to[c] + v;
+      }
+    });
+#pragma unroll
+    for (int c = 0; c < 4; ++c) {
+      if (c >= ch.C) break;
+      if (HAS_QU && c == ch.q)
+        acc[c] += tq * bv;
+      else if (HAS_QU && c == ch.u)
+        acc[c] += tu * bv;
+      else
+        acc[c] += to[c] * bv;
+    }
+  } else {
+    // nearest: unclamped z; |z| > 1 makes the reference's ring_above NaN-based
+    // and the clamp then picks ring 1 (numba_healpy.py:62-70, tod_nearest.py:115-120)
+    const double sin_th = sqrt(max0(vx * vx + vy * vy));
+    int ir_above;
+    if (fabs(vz) <= 1.0) {
+      ir_above = ring_above_fast(nside, vz);
+      ir_above = ir_above < 1 ? 1 : (ir_above > 4 * nside - 2 ? 4 * nside - 2 : ir_above);
+    } else {
+      ir_above = 1;
+    }
+    int best_pix = 0, best_ring = 0, best_ip = 0, best_n = 1;
+    double best_cos = -2.0, best_zc = 0.0, best_phic = 0.0;
+#pragma unroll
+    for (int g = 0; g < 2; ++g) {
+      const int ir = ir_above + g;
+      const RingRec* rr = rt + ir;
+      const int n = __ldg(&rr->n);
+      const double phi0 = __ldg(&rr->phi0), dphi = __ldg(&rr->dphi), zc = __ldg(&rr->z), szc = __ldg(&rr->sth);
+      int ipb = (int)(phi_w * (double)n / kTwoPi);
+      if (ipb >= n) ipb -= n;
+#pragma unroll
+      for (int t = 0; t < 2; ++t) {
+        const int ip = (t == 0) ? ipb : wrap_up(ipb, 1, n);
+        const double phic = phi0 + (double)ip * dphi;
+        const double cosd = sin_th * szc * cos(phi_w - phic) + vz * zc;
+        if (cosd > best_cos) {
+          best_cos = cosd;
+          best_pix = (int)__ldg(&rr->first) + ip;
+          best_ring = ir;
+          best_ip = ip;
+          best_n = n;
+          best_zc = zc;
+          best_phic = phic;
+        }
+      }
+    }
+    if constexpr (HAS_QU) {
+      double c2d, s2d;
+      spin2_fast(w, tab, best_ring, best_ip, best_n, best_zc, best_phic, bo, c2d, s2d);
+      const double qv = map_i<MapT>(a, ch.q, best_pix);
+      const double uv = map_i<MapT>(a, ch.u, best_pix);
+#pragma unroll
+      for (int c = 0; c < 4; ++c) {
+        if (c >= ch.C) break;
+        if (c == ch.q)
+          acc[c] += (qv * c2d + uv * s2d) * bv;
+        else if (c == ch.u)
+          acc[c] += (-qv * s2d + uv * c2d) * bv;
+        else
+          acc[c] += map_x_beam_i<MapT>(a, c, best_pix, bvf);
+      }
+    } else {
+#pragma unroll
+      for (int c = 0; c < 4; ++c) {
+        if (c >= ch.C) break;
+        acc[c] += map_x_beam_i<MapT>(a, c, best_pix, bvf);
       }
     }
   }
@@ -413,9 +645,7 @@ __device__ __forceinline__ void eval_pixel(const KArgs& a, const SampleRot& rot,
 // Flush the per-warp partial sums of sample `b` into tod (fixed order).
 template <int NW>
 __device__ __forceinline__ void flush_sample(const KArgs& a, const double* s_red, long long b) {
-#pragma unroll
-  for (int c = 0; c < 4; ++c) {
-    if (c >= a.C) break;
+  for (int c = 0; c < a.C; ++c) {
     double v = 0.0;
     for (int i = 0; i < NW; ++i) v += s_red[i * 4 + c];
     a.tod[(long long)c * a.tod_stride + b] += v;
@@ -425,9 +655,10 @@ __device__ __forceinline__ void flush_sample(const KArgs& a, const double* s_red
 // Main kernel.  With a ring table: ring data come from it and, when the
 // entry carries Q and U, each sample's footprint gets a spin-2 table in
 // shared memory.  Without one: everything is evaluated directly.
-template <int MODE, bool HAS_QU, typename MapT, bool P64, int NT, int MINB>
+template <int MODE, bool HAS_QU, typename MapT, bool P64, int LAYOUT, int NT, int MINB>
 __global__ void __launch_bounds__(NT, MINB) gather_accum_kernel(const KArgs a) {
   constexpr int NW = NT / 32;
+  constexpr int kSetupThreads = 64;  // threads that derive a sample's footprint window
   extern __shared__ __align__(16) unsigned char smem_raw[];
   Spin2Tab& w = *reinterpret_cast<Spin2Tab*>(smem_raw);
   double2* tab = reinterpret_cast<double2*>(smem_raw + ((sizeof(Spin2Tab) + 15) & ~size_t(15)));
@@ -435,6 +666,7 @@ __global__ void __launch_bounds__(NT, MINB) gather_accum_kernel(const KArgs a) {
 
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const RingRec* rt = static_cast<const RingRec*>(a.ring_table);
+  const bool fast = rt != nullptr && a.nside <= 8192;
   double cx = 0.0, cy = 0.0, cz = 1.0, reach = 0.0;
   bool use_tab = false;
   if (rt != nullptr && HAS_QU) {
@@ -448,6 +680,8 @@ __global__ void __launch_bounds__(NT, MINB) gather_accum_kernel(const KArgs a) {
   if (threadIdx.x == 0) {
     w.nr = 0;
     w.total = 0;
+    w.ir_lo = 0;
+    w.ir_lo32 = 0;
   }
   unsigned long long nerr = 0;
   long long prev = -1;
@@ -458,44 +692,47 @@ __global__ void __launch_bounds__(NT, MINB) gather_accum_kernel(const KArgs a) {
     __syncthreads();  // previous sample is done with the table and its partial sums
     if (prev >= 0 && threadIdx.x == 0) flush_sample<NW>(a, s_red, prev);
     if (use_tab) {
-      // footprint window of this sample (same values in every thread)
-      double ux, uy, uz;
-      rot_f64(rot, cx, cy, cz, ux, uy, uz);
-      const double theta_u = acos(clamp1(uz));
-      double phi_u = atan2(uy, ux);
-      if (phi_u < 0.0) phi_u += kTwoPi;
-      const double th_lo = theta_u - reach, th_hi = theta_u + reach;
-      long long ir_lo = th_lo <= 0.0 ? 1 : hp_ring_above(a.nside, cos(th_lo));
-      long long ir_hi = th_hi >= kPi ? 4 * a.nside - 1 : hp_ring_above(a.nside, cos(th_hi)) + 1;
-      ir_lo = max(ir_lo, 1LL);
-      ir_hi = min(ir_hi, 4 * a.nside - 1);
-      // a non-finite footprint centre gives an empty or invalid window: no table
-      const long long nr = ir_hi - ir_lo + 1;
-      bool fits = nr > 0 && nr <= kRingCap && ir_lo >= 1 && ir_hi <= 4 * a.nside - 1;
-      long long base = 0, total = 0;
-      if (fits) {
-        base = __ldg(&rt[ir_lo].pre);
-        total = __ldg(&rt[ir_hi].pre) + __ldg(&rt[ir_hi].cap) - base;
-        fits = total <= a.tab_cap;
-      }
-      if (fits) {
-        for (int t = threadIdx.x; t < nr; t += NT) {
-          const RingRec* r = rt + ir_lo + t;
-          const int n = __ldg(&r->n), cap = __ldg(&r->cap);
-          int iplo = 0;
-          if (cap < n) {
-            const double c = floor((phi_u - __ldg(&r->phi0)) / __ldg(&r->dphi));
-            iplo = (int)py_imod((long long)c - (cap - 1) / 2, n);
-          }
-          w.off[t] = (int)(__ldg(&r->pre) - base);
-          w.iplo[t] = iplo;
-          w.cap[t] = cap;
+      if (threadIdx.x < kSetupThreads) {
+        // footprint window of this sample (same values in every setup thread)
+        double ux, uy, uz;
+        rot_f64(rot, cx, cy, cz, ux, uy, uz);
+        const double theta_u = acos(clamp1(uz));
+        double phi_u = atan2(uy, ux);
+        if (phi_u < 0.0) phi_u += kTwoPi;
+        const double th_lo = theta_u - reach, th_hi = theta_u + reach;
+        long long ir_lo = th_lo <= 0.0 ? 1 : hp_ring_above(a.nside, cos(th_lo));
+        long long ir_hi = th_hi >= kPi ? 4 * a.nside - 1 : hp_ring_above(a.nside, cos(th_hi)) + 1;
+        ir_lo = max(ir_lo, 1LL);
+        ir_hi = min(ir_hi, 4 * a.nside - 1);
+        // a non-finite footprint centre gives an empty or invalid window: no table
+        const long long nr = ir_hi - ir_lo + 1;
+        bool fits = nr > 0 && nr <= kRingCap && ir_lo >= 1 && ir_hi <= 4 * a.nside - 1;
+        long long base = 0, total = 0;
+        if (fits) {
+          base = __ldg(&rt[ir_lo].pre);
+          total = __ldg(&rt[ir_hi].pre) + __ldg(&rt[ir_hi].cap) - base;
+          fits = total <= a.tab_cap;
         }
-      }
-      if (threadIdx.x == 0) {
-        w.ir_lo = ir_lo;
-        w.nr = fits ? (int)nr : 0;
-        w.total = fits ? (int)total : 0;
+        if (fits) {
+          for (int t = threadIdx.x; t < nr; t += kSetupThreads) {
+            const RingRec* r = rt + ir_lo + t;
+            const int n = __ldg(&r->n), cap = __ldg(&r->cap);
+            int iplo = 0;
+            if (cap < n) {
+              const double c = floor((phi_u - __ldg(&r->phi0)) / __ldg(&r->dphi));
+              iplo = (int)py_imod((long long)c - (cap - 1) / 2, n);
+            }
+            w.off[t] = (int)(__ldg(&r->pre) - base);
+            w.iplo[t] = iplo;
+            w.cap[t] = cap;
+          }
+        }
+        if (threadIdx.x == 0) {
+          w.ir_lo = ir_lo;
+          w.ir_lo32 = (int)ir_lo;
+          w.nr = fits ? (int)nr : 0;
+          w.total = fits ? (int)total : 0;
+        }
       }
       __syncthreads();
       const int ntab = w.total, nwin = w.nr;
@@ -521,14 +758,20 @@ __global__ void __launch_bounds__(NT, MINB) gather_accum_kernel(const KArgs a) {
     __syncthreads();
 
     double acc[4] = {0.0, 0.0, 0.0, 0.0};
-    if (rt != nullptr) {
-      const TableRings rings{rt};
-      for (long long s = threadIdx.x; s < a.S; s += NT)
-        eval_pixel<MODE, HAS_QU, MapT, P64>(a, rot, bo, rings, w, tab, s, acc, nerr);
-    } else {
-      const DirectRings rings{a.nside, a.npix};
-      for (long long s = threadIdx.x; s < a.S; s += NT)
-        eval_pixel<MODE, HAS_QU, MapT, P64>(a, rot, bo, rings, w, tab, s, acc, nerr);
+    for (long long s = threadIdx.x; s < a.S; s += NT) {
+      double vx, vy, vz;
+      rotate_pixel<P64>(a, rot, s, vx, vy, vz);
+      const float bvf = __ldg(a.beam + s);
+      double phi_w = atan2(vy, vx);
+      if (phi_w < 0.0) phi_w += kTwoPi;
+      if (fast && isfinite(vx) && isfinite(vy) && isfinite(vz)) {
+        eval_fast<MODE, HAS_QU, MapT, LAYOUT>(a, bo, rt, w, tab, vx, vy, vz, phi_w, bvf, acc);
+      } else if (rt != nullptr) {
+        eval_generic<MODE, HAS_QU, MapT, P64>(a, bo, TableRings{rt}, w, tab, vx, vy, vz, phi_w, bvf, acc, nerr);
+      } else {
+        eval_generic<MODE, HAS_QU, MapT, P64>(a, bo, DirectRings{a.nside, a.npix}, w, tab, vx, vy, vz, phi_w, bvf,
+                                              acc, nerr);
+      }
     }
 #pragma unroll
     for (int c = 0; c < 4; ++c) {
@@ -777,6 +1020,26 @@ __global__ void spin2_kernel(const double* zp, const double* sp, const double* p
   }
 }
 
+// FP64 pipe throughput probe: 8 independent FMA chains per thread, so the
+// pipe, not latency, bounds it.  flops = 2 * 8 * iters per thread.
+__global__ void fp64_probe_kernel(int iters, double seed, double* out) {
+  double a0 = seed + threadIdx.x, a1 = a0 + 1, a2 = a0 + 2, a3 = a0 + 3, a4 = a0 + 4, a5 = a0 + 5, a6 = a0 + 6,
+         a7 = a0 + 7;
+  const double m = 0.999999, c = 1e-7;
+  for (int i = 0; i < iters; ++i) {
+    a0 = fma(a0, m, c);
+    a1 = fma(a1, m, c);
+    a2 = fma(a2, m, c);
+    a3 = fma(a3, m, c);
+    a4 = fma(a4, m, c);
+    a5 = fma(a5, m, c);
+    a6 = fma(a6, m, c);
+    a7 = fma(a7, m, c);
+  }
+  const double v = ((a0 + a1) + (a2 + a3)) + ((a4 + a5) + (a6 + a7));
+  if (v == 12345.678) out[blockIdx.x] = v;  // keeps the chains alive; never true in practice
+}
+
 // ---------------------------------------------------------------------------
 // Host side.
 // ---------------------------------------------------------------------------
@@ -807,9 +1070,9 @@ constexpr size_t kTabHeaderBytes = (sizeof(Spin2Tab) + 15) & ~size_t(15);
 constexpr int kNT = TODGPU_CTA_THREADS;  // threads per CTA
 constexpr int kMinB = TODGPU_CTA_MINB;   // CTAs per SM the register budget is sized for
 
-template <int MODE, bool HAS_QU, typename MapT, bool P64>
+template <int MODE, bool HAS_QU, typename MapT, bool P64, int LAYOUT>
 static int launch_gather(KArgs k, cudaStream_t stream) {
-  auto kern = gather_accum_kernel<MODE, HAS_QU, MapT, P64, kNT, kMinB>;
+  auto kern = gather_accum_kernel<MODE, HAS_QU, MapT, P64, LAYOUT, kNT, kMinB>;
   static LaunchInfo info;
   static std::mutex mu;
   const int tab_cap = (HAS_QU && k.ring_table != nullptr) ? kTabCapDefault : 0;
@@ -838,7 +1101,9 @@ static int launch_gather(KArgs k, cudaStream_t stream) {
 
 template <int MODE, typename MapT, bool P64>
 static int dispatch_qu(const KArgs& k, bool has_qu, cudaStream_t s) {
-  return has_qu ? launch_gather<MODE, true, MapT, P64>(k, s) : launch_gather<MODE, false, MapT, P64>(k, s);
+  if (has_qu && k.C == 3 && k.c_q == 1 && k.c_u == 2) return launch_gather<MODE, true, MapT, P64, kLayoutIQU>(k, s);
+  return has_qu ? launch_gather<MODE, true, MapT, P64, kLayoutGeneric>(k, s)
+                : launch_gather<MODE, false, MapT, P64, kLayoutGeneric>(k, s);
 }
 
 template <int MODE>
@@ -1038,6 +1303,15 @@ extern "C" int todgpu_ring_table_build(int64_t nside, double reach, void* table,
   ring_prefix_kernel<<<1, 1024, 0, s>>>(nside, t);
   cudaError_t e = cudaGetLastError();
   return e == cudaSuccess ? TODGPU_OK : cuda_fail(e, "ring table kernels");
+}
+
+extern "C" int todgpu_fp64_probe(int64_t blocks, int32_t iters, double* sink, double* flops, void* stream) {
+  if (blocks < 1 || iters < 1 || !sink || !flops) return fail(TODGPU_EINVAL, "bad probe arguments");
+  fp64_probe_kernel<<<(unsigned)blocks, 256, 0, static_cast<cudaStream_t>(stream)>>>(iters, 0.5, sink);
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return cuda_fail(e, "fp64_probe_kernel launch");
+  *flops = 2.0 * 8.0 * (double)iters * 256.0 * (double)blocks;
+  return TODGPU_OK;
 }
 
 extern "C" int todgpu_abi_version(void) { return TODGPU_ABI_VERSION; }

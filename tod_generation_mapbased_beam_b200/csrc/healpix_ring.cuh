@@ -66,6 +66,19 @@ __device__ __forceinline__ double clamp1(double x) {
   return (a > -1.0) ? a : -1.0;
 }
 
+// theta_q - theta_a for a query z and a nearby ring (z_a, s_a = sin theta_a):
+// sin(theta_q - theta_a) = z_a sin(theta_q) - z sin(theta_a), and for |d| <
+// 0.01 asin(d) = d + d^3/6 + 3 d^5/40 + 5 d^7/112 (the next term is below
+// 3e-20).  Returns false when the angle is too large for the series.
+__device__ __forceinline__ bool dtheta_small(double z, double za, double sa, double& out) {
+  const double sq = sqrt((1.0 - z) * (1.0 + z));
+  const double d = fma(za, sq, -z * sa);
+  if (!(fabs(d) < 0.01)) return false;
+  const double d2 = d * d;
+  out = fma(d * d2, fma(d2, fma(d2, 5.0 / 112.0, 3.0 / 40.0), 1.0 / 6.0), d);
+  return true;
+}
+
 // Index of the last ring whose centre z is > z (1-based; 0 above ring 1).
 __device__ __forceinline__ long long hp_ring_above(long long nside, double z) {
   double az = fabs(z);
@@ -207,8 +220,9 @@ __device__ __forceinline__ void hp_stencil(long long nside, double z, double phi
   } else {
     const RingData ra = rings(ir_above);
     const RingData rb = rings(ir_below);
-    const double theta = acos(z);
-    const double wb = (theta - ra.ta) / (rb.ta - ra.ta);
+    double dta;
+    if (!dtheta_small(z, ra.z, rings.sth(ir_above, ra), dta)) dta = acos(z) - ra.ta;
+    const double wb = dta / (rb.ta - ra.ta);
     const double wa = 1.0 - wb;
     double tw = py_fmod_pos((phi_w - ra.phi0) / ra.dphi, (double)ra.n);
     const long long ia = py_int(tw);
@@ -281,7 +295,10 @@ __device__ __forceinline__ Nearest hp_nearest(long long nside, double z, double 
 }
 
 // cos 2d, sin 2d of the frame rotation between a pixel centre and the
-// boresight (tan d = N/D from the haversine form; identity for equal points).
+// boresight (tan d = N/D from the haversine form; identity for equal points),
+// tod_bilinear.py:84-145.  Evaluated in the reference's exact operation order
+// (no contraction): near the poles D is a difference of nearly equal terms,
+// so any reassociation moves the result by far more than an ulp.
 __device__ __forceinline__ void spin2_c2s2(double z_pix, double sth_pix, double phi_pix, double z_pts,
                                            double sth_pts, double phi_pts, double& c2d, double& s2d) {
   if (phi_pts == phi_pix && sth_pts == sth_pix && z_pts == z_pix) {

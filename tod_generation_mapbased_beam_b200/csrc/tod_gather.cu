@@ -349,15 +349,15 @@ __device__ __noinline__ void eval_generic(const KArgs& a, const Bore& bo, const 
                    spin2_lookup(w, tab, ring, ip, n, zn, phin, bo, c2, s2);
                    const double q = map_at<MapT>(a, a.c_q, p);
                    const double u = map_at<MapT>(a, a.c_u, p);
-                   const double vq = wk * (q * c2 + u * s2);
-                   const double vu = wk * (-q * s2 + u * c2);
+                   const double vq = wk * fma(q, c2, u * s2);
+                   const double vu = wk * fma(u, c2, -q * s2);
                    tq = (k == 0) ? vq : tq + vq;
                    tu = (k == 0) ? vu : tu + vu;
                  }
                  for (int c = 0; c < a.C; ++c) {
                    if (HAS_QU && (c == a.c_q || c == a.c_u)) continue;
-                   const double v = wk * map_at<MapT>(a, c, p);
-                   to[c] = (k == 0) ? v : to[c] + v;
+                   const double m = map_at<MapT>(a, c, p);
+                   to[c] = (k == 0) ? wk * m : fma(wk, m, to[c]);
                  }
                });
     if (!ok) {
@@ -366,11 +366,11 @@ __device__ __noinline__ void eval_generic(const KArgs& a, const Bore& bo, const 
     }
     for (int c = 0; c < a.C; ++c) {
       if (HAS_QU && c == a.c_q)
-        acc[c] += tq * bv;
+        acc[c] = fma(tq, bv, acc[c]);
       else if (HAS_QU && c == a.c_u)
-        acc[c] += tu * bv;
+        acc[c] = fma(tu, bv, acc[c]);
       else
-        acc[c] += to[c] * bv;
+        acc[c] = fma(to[c], bv, acc[c]);
     }
   } else {
     const double sin_th = sqrt(max0(vx * vx + vy * vy));
@@ -386,9 +386,9 @@ __device__ __noinline__ void eval_generic(const KArgs& a, const Bore& bo, const 
       const double uv = map_at<MapT>(a, a.c_u, nb.pix);
       for (int c = 0; c < a.C; ++c) {
         if (c == a.c_q)
-          acc[c] += (qv * c2d + uv * s2d) * bv;
+          acc[c] = fma(fma(qv, c2d, uv * s2d), bv, acc[c]);
         else if (c == a.c_u)
-          acc[c] += (-qv * s2d + uv * c2d) * bv;
+          acc[c] = fma(fma(uv, c2d, -qv * s2d), bv, acc[c]);
         else
           acc[c] += map_x_beam<MapT>(a, c, nb.pix, bvf);
       }
@@ -479,8 +479,9 @@ __device__ __forceinline__ void stencil_fast(int nside, double z, double phi_w, 
     const int ir_below = ir_above + 1;
     const RingFast ra = ring_fast(rt, ir_above);
     const RingFast rb = ring_fast(rt, ir_below);
-    const double theta = acos(z);
-    const double wb = (theta - ra.ta) / (rb.ta - ra.ta);
+    double dta;
+    if (!dtheta_small(z, ra.z, __ldg(&rt[ir_above].sth), dta)) dta = acos(z) - ra.ta;
+    const double wb = dta / (rb.ta - ra.ta);
     const double wa = 1.0 - wb;
     double tw = py_fmod_pos((phi_w - ra.phi0) / ra.dphi, (double)ra.n);
     const int ia = (int)tw;
@@ -557,8 +558,8 @@ __device__ __forceinline__ void eval_fast(const KArgs& a, const Bore& bo, const 
         spin2_fast(w, tab, ring, ip, n, zn, phin, bo, c2, s2);
         const double q = map_i<MapT>(a, ch.q, p);
         const double u = map_i<MapT>(a, ch.u, p);
-        const double vq = wk * (q * c2 + u * s2);
-        const double vu = wk * (-q * s2 + u * c2);
+        const double vq = wk * fma(q, c2, u * s2);
+        const double vu = wk * fma(u, c2, -q * s2);
         tq = (k == 0) ? vq : tq + vq;
         tu = (k == 0) ? vu : tu + vu;
       }
@@ -566,19 +567,19 @@ __device__ __forceinline__ void eval_fast(const KArgs& a, const Bore& bo, const 
       for (int c = 0; c < 4; ++c) {
         if (c >= ch.C) break;
         if (HAS_QU && (c == ch.q || c == ch.u)) continue;
-        const double v = wk * map_i<MapT>(a, c, p);
-        to[c] = (k == 0) ? v : to[c] + v;
+        const double m = map_i<MapT>(a, c, p);
+        to[c] = (k == 0) ? wk * m : fma(wk, m, to[c]);
       }
     });
 #pragma unroll
     for (int c = 0; c < 4; ++c) {
       if (c >= ch.C) break;
       if (HAS_QU && c == ch.q)
-        acc[c] += tq * bv;
+        acc[c] = fma(tq, bv, acc[c]);
       else if (HAS_QU && c == ch.u)
-        acc[c] += tu * bv;
+        acc[c] = fma(tu, bv, acc[c]);
       else
-        acc[c] += to[c] * bv;
+        acc[c] = fma(to[c], bv, acc[c]);
     }
   } else {
     // nearest: unclamped z; |z| > 1 makes the reference's ring_above NaN-based
@@ -626,9 +627,9 @@ __device__ __forceinline__ void eval_fast(const KArgs& a, const Bore& bo, const 
       for (int c = 0; c < 4; ++c) {
         if (c >= ch.C) break;
         if (c == ch.q)
-          acc[c] += (qv * c2d + uv * s2d) * bv;
+          acc[c] = fma(fma(qv, c2d, uv * s2d), bv, acc[c]);
         else if (c == ch.u)
-          acc[c] += (-qv * s2d + uv * c2d) * bv;
+          acc[c] = fma(fma(uv, c2d, -qv * s2d), bv, acc[c]);
         else
           acc[c] += map_x_beam_i<MapT>(a, c, best_pix, bvf);
       }
@@ -658,12 +659,12 @@ __device__ __forceinline__ void flush_sample(const KArgs& a, const double* s_red
 template <int MODE, bool HAS_QU, typename MapT, bool P64, int LAYOUT, int NT, int MINB>
 __global__ void __launch_bounds__(NT, MINB) gather_accum_kernel(const KArgs a) {
   constexpr int NW = NT / 32;
-  constexpr int kSetupThreads = 64;  // threads that derive a sample's footprint window
   extern __shared__ __align__(16) unsigned char smem_raw[];
   Spin2Tab& w = *reinterpret_cast<Spin2Tab*>(smem_raw);
   double2* tab = reinterpret_cast<double2*>(smem_raw + ((sizeof(Spin2Tab) + 15) & ~size_t(15)));
   __shared__ double s_red[NW * 4];
 
+  constexpr int kSetupThreads = 64;  // threads that derive a sample's footprint window
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const RingRec* rt = static_cast<const RingRec*>(a.ring_table);
   const bool fast = rt != nullptr && a.nside <= 8192;
@@ -672,9 +673,13 @@ __global__ void __launch_bounds__(NT, MINB) gather_accum_kernel(const KArgs a) {
   if (rt != nullptr && HAS_QU) {
     double rbeam;
     beam_extent<P64, NT>(a, s_red, cx, cy, cz, rbeam);
-    // stencil neighbours lie within ~3 pixel sizes of the query: 4/nside
-    // rad, plus slack for the float32 parameter rounding
-    reach = rbeam + 4.0 / (double)a.nside + 1e-5;
+    // every stencil neighbour centre lies within 1.7/nside rad of the query
+    // (one ring spacing plus one pixel width; the opposite pair around a pole
+    // within twice the colatitude of ring 1); 3/nside leaves margin, plus
+    // slack for the float32 parameter rounding.  A neighbour outside the
+    // window is still evaluated correctly (directly), only slower.
+    reach = rbeam + 3.0 / (double)a.nside + 1e-5;
+    // the ring table reserves per-ring slots for footprints up to its reach
     use_tab = reach <= __ldg(&rt[0].ta);
   }
   if (threadIdx.x == 0) {

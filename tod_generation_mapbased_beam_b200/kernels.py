@@ -64,7 +64,9 @@ _REACH_STEP = 1e-4  # ring tables are built for reaches rounded up to this step 
 def beam_reach(vec_orig, nside):
     """Angular radius [rad] that every stencil neighbour of the rotated beam
     stays within around the rotated beam centre: the beam's radius about its
-    mean direction plus 4/nside (stencil reach) plus float32 slack."""
+    mean direction plus 3/nside (stencil reach) plus float32 slack.  The
+    kernel derives the same bound from the beam on the device and uses the
+    ring table's spin-2 slots only if the table covers it."""
     v = vec_orig.detach().cpu().numpy() if is_tensor(vec_orig) else np.asarray(vec_orig)
     v = np.asarray(v, np.float64).reshape(-1, 3)
     if v.shape[0] == 0:
@@ -76,7 +78,7 @@ def beam_reach(vec_orig, nside):
     with np.errstate(invalid="ignore", divide="ignore"):
         d = np.where(vn > 0, (v @ c) / vn, -1.0)
     r = float(np.arccos(np.clip(d.min(), -1.0, 1.0)))
-    return r + 4.0 / float(nside) + 2e-5
+    return r + 3.0 / float(nside) + 2e-5
 
 
 def ring_table(nside, reach, device=None):

@@ -98,6 +98,23 @@ typedef struct todgpu_gather_args {
  * and tod_nearest._gather_accum_nearest_jit (tod_nearest.py:21-158). */
 int todgpu_gather_accum(const todgpu_gather_args *args, void *stream);
 
+/* The same fused gather/accumulate as todgpu_gather_accum, for callers that
+ * cannot allocate device memory themselves -- for example a host application
+ * whose device memory is owned by another framework's allocator, or a foreign-
+ * language binding that can hand over existing buffers but has no way to
+ * create new ones.  Instead of a caller-provided ring table it uses one built
+ * into the library: a statically sized array (1 MiB, nside <= 4096) that every
+ * GPU loading the library holds until the process exits.  args->ring_table is
+ * ignored; nside > 4096 is rejected with TODGPU_ENSIDE.  Each call rebuilds
+ * the table on `stream` for its own nside and beam before the gather, so no
+ * state carries over between calls, but all calls share the one array: calls
+ * that can overlap on the GPU (different streams or host threads) race and
+ * must be serialised by the caller.  The first call on a device looks up the
+ * array's device address (cudaGetSymbolAddress); make that first call before
+ * any stream capture.  It allocates nothing.  No counterpart in the
+ * reference. */
+int todgpu_gather_accum_static(const todgpu_gather_args *args, void *stream);
+
 /* Per-(b, s) bilinear stencil of the fused path: pix (4, B*S) int64 and
  * wgt (4, B*S) float64 with n = b*S + s.  Replaces the split reference path
  * tod_rotations._rodrigues_jit (tod_rotations.py:33-80) + vec2ang +

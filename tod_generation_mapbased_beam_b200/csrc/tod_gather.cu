@@ -43,6 +43,7 @@ namespace todgpu {
 constexpr int kRingCap = 192;   // rings per footprint window
 constexpr int kTabCapDefault = 2048;  // spin-2 table slots per sample (32 KB)
 constexpr long long kMaxNside = 16384;
+constexpr int kNTStatic = 256;  // threads of the reach kernel of the built-in table
 
 thread_local std::string g_last_error;
 
@@ -800,9 +801,10 @@ __global__ void __launch_bounds__(NT, MINB) gather_accum_kernel(const KArgs a) {
 // radius `reach`: a disc meets the latitude of the ring in a longitude
 // interval of half-width at most asin(sin(reach) / sin(theta_r)), or the
 // whole ring when the disc can contain the pole.
-__global__ void ring_table_kernel(long long nside, double reach, RingRec* t) {
+__global__ void ring_table_kernel(long long nside, double reach, RingRec* t, bool reach_from_header) {
   const long long nrings = 4 * nside - 1;
   const long long npix = 12 * nside * nside;
+  if (reach_from_header) reach = t[0].ta;
   for (long long ir = 1 + blockIdx.x * (long long)blockDim.x + threadIdx.x; ir <= nrings;
        ir += (long long)gridDim.x * blockDim.x) {
     const RingInfo ri = hp_ring_info(nside, ir, npix);
@@ -827,7 +829,7 @@ __global__ void ring_table_kernel(long long nside, double reach, RingRec* t) {
     r.pre = 0;
     t[ir] = r;
   }
-  if (blockIdx.x == 0 && threadIdx.x == 0) {
+  if (!reach_from_header && blockIdx.x == 0 && threadIdx.x == 0) {
     RingRec h;
     h.z = (double)nside;
     h.ta = reach;
@@ -1025,6 +1027,37 @@ __global__ void spin2_kernel(const double* zp, const double* sp, const double* p
   }
 }
 
+// ---------------------------------------------------------------------------
+// Built-in ring table for callers that cannot allocate device memory.
+// ---------------------------------------------------------------------------
+
+// Largest nside the built-in table holds: 4 * 4096 records of 64 bytes = 1 MiB,
+// resident on every GPU that loads the library until the process exits.
+constexpr long long kStaticMaxNside = 4096;
+static __device__ __align__(256) RingRec g_static_ring_table[4 * kStaticMaxNside];
+
+// Header of a table built from the beam on the device: the footprint reach the
+// gather kernel derives from the same beam (same code, plus a hair of margin).
+template <bool P64>
+__global__ void __launch_bounds__(kNTStatic) static_reach_kernel(const KArgs a, RingRec* t) {
+  __shared__ double s_red[(kNTStatic / 32) * 4];
+  double cx, cy, cz, rbeam;
+  beam_extent<P64, kNTStatic>(a, s_red, cx, cy, cz, rbeam);
+  if (threadIdx.x == 0) {
+    RingRec h;
+    h.z = (double)a.nside;
+    h.ta = rbeam + 3.0 / (double)a.nside + 1e-5 + 1e-9;
+    h.sth = 0.0;
+    h.phi0 = 0.0;
+    h.dphi = 0.0;
+    h.first = 0;
+    h.n = 0;
+    h.cap = 0;
+    h.pre = 0;
+    t[0] = h;
+  }
+}
+
 // FP64 pipe throughput probe: 8 independent FMA chains per thread, so the
 // pipe, not latency, bounds it.  flops = 2 * 8 * iters per thread.
 __global__ void fp64_probe_kernel(int iters, double seed, double* out) {
@@ -1202,6 +1235,59 @@ extern "C" int todgpu_gather_accum(const todgpu_gather_args* a, void* stream) {
   return dispatch_types<TODGPU_NEAREST>(k, has_qu, a->map_dtype, a->params_dtype, s);
 }
 
+// Device address of the built-in ring table on the current device, looked up
+// once per device (cudaGetSymbolAddress with that device current).
+static int static_table_ptr(RingRec** out) {
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return cuda_fail(e, "cudaGetDevice");
+  static std::mutex mu;
+  static std::vector<RingRec*> ptrs;
+  std::lock_guard<std::mutex> lock(mu);
+  if ((int)ptrs.size() <= dev) ptrs.resize(dev + 1, nullptr);
+  if (ptrs[dev] == nullptr) {
+    void* p = nullptr;
+    e = cudaGetSymbolAddress(&p, g_static_ring_table);
+    if (e != cudaSuccess) return cuda_fail(e, "cudaGetSymbolAddress(g_static_ring_table)");
+    ptrs[dev] = static_cast<RingRec*>(p);
+  }
+  *out = ptrs[dev];
+  return TODGPU_OK;
+}
+
+extern "C" int todgpu_gather_accum_static(const todgpu_gather_args* a, void* stream) {
+  int rc = check_common(a, true);
+  if (rc != TODGPU_OK) return rc;
+  if (a->nside > kStaticMaxNside)
+    return fail(TODGPU_ENSIDE, "nside " + std::to_string(a->nside) +
+                                   " exceeds 4096, the largest nside of the built-in ring table; use "
+                                   "todgpu_gather_accum with a caller-allocated table");
+  if (a->B == 0 || a->S == 0) return TODGPU_OK;
+  RingRec* t = nullptr;
+  rc = static_table_ptr(&t);
+  if (rc != TODGPU_OK) return rc;
+  KArgs k = make_kargs(a);
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  if (!(a->flags & TODGPU_FLAG_NO_TABLES)) {
+    // every call rebuilds the whole table (header, records, prefix sums) for
+    // its own nside and beam, so nothing depends on earlier contents
+    if (a->params_dtype == TODGPU_F32)
+      static_reach_kernel<false><<<1, kNTStatic, 0, s>>>(k, t);
+    else
+      static_reach_kernel<true><<<1, kNTStatic, 0, s>>>(k, t);
+    ring_table_kernel<<<grid_for(4 * a->nside, 256), 256, 0, s>>>(a->nside, 0.0, t, true);
+    ring_prefix_kernel<<<1, 1024, 0, s>>>(a->nside, t);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return cuda_fail(e, "built-in ring table kernels");
+    k.ring_table = t;
+  } else {
+    k.ring_table = nullptr;
+  }
+  const bool has_qu = (a->c_q >= 0 && a->c_u >= 0);
+  if (a->interp == TODGPU_BILINEAR) return dispatch_types<TODGPU_BILINEAR>(k, has_qu, a->map_dtype, a->params_dtype, s);
+  return dispatch_types<TODGPU_NEAREST>(k, has_qu, a->map_dtype, a->params_dtype, s);
+}
+
 extern "C" int todgpu_bilinear_stencils(const todgpu_gather_args* a, int64_t* pix, double* wgt, void* stream) {
   int rc = check_common(a, false);
   if (rc != TODGPU_OK) return rc;
@@ -1304,7 +1390,7 @@ extern "C" int todgpu_ring_table_build(int64_t nside, double reach, void* table,
   if (!(reach >= 0.0) || !(reach <= kPi)) return fail(TODGPU_EINVAL, "reach must be in [0, pi]");
   cudaStream_t s = static_cast<cudaStream_t>(stream);
   RingRec* t = static_cast<RingRec*>(table);
-  ring_table_kernel<<<grid_for(4 * nside, 256), 256, 0, s>>>(nside, reach, t);
+  ring_table_kernel<<<grid_for(4 * nside, 256), 256, 0, s>>>(nside, reach, t, false);
   ring_prefix_kernel<<<1, 1024, 0, s>>>(nside, t);
   cudaError_t e = cudaGetLastError();
   return e == cudaSuccess ? TODGPU_OK : cuda_fail(e, "ring table kernels");

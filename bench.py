@@ -46,6 +46,12 @@ sys.path.insert(0, ROOT)
 
 METRIC = "TOD samples/s, 1 B200: FP64 plain vs mixed/learned-tail at fixed RMS error"
 
+# FP64 flops per (sample, beam pixel) evaluation of the reference algorithm,
+# counted by ncu on the direct-evaluation path (TODGPU_FLAG_NO_TABLES) of the
+# config-2 workload: dadd + dmul + 2 * dfma per evaluation
+# (profiles/gather_accum_bilinear_config2.md).
+FLOPS_PER_EVAL = {"bilinear": 853.0, "nearest": 853.0}
+
 
 def parse_args():
     p = argparse.ArgumentParser()
@@ -258,6 +264,31 @@ def measured_peaks():
         return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0}, "fallback"
 
 
+def fp64_peak_tflops():
+    """FP64 FMA throughput of this GPU, measured with the library's probe."""
+    import torch
+
+    from tod_generation_mapbased_beam_b200 import _native
+
+    lib = _native.lib()
+    sms = torch.cuda.get_device_properties(torch.cuda.current_device()).multi_processor_count
+    blocks = sms * 16
+    sink = torch.zeros(blocks, dtype=torch.float64, device="cuda")
+    flops = ctypes.c_double()
+    stream = torch.cuda.current_stream()
+    best = 0.0
+    for _ in range(4):
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        _native.check(lib.todgpu_fp64_probe(blocks, 4096, sink.data_ptr(), ctypes.byref(flops),
+                                            stream.cuda_stream))
+        e1.record(stream)
+        e1.synchronize()
+        best = max(best, flops.value / (e0.elapsed_time(e1) / 1e3) / 1e12)
+    return best
+
+
 def profiled_traffic(mode):
     """dram bytes per launch recorded by the committed ncu summary, if any."""
     path = os.path.join(ROOT, "profiles", f"gather_accum_{mode}_config2.md")
@@ -331,18 +362,28 @@ def run_ours(args, dist):
     kernel_ms = dist.max(statistics.mean(kern_ms))
     value = B * dist.world * args.steps / (total_ms / 1e3)
 
-    # roofline of the fused kernel (compulsory DRAM bytes per launch)
+    # roofline of the fused kernel: FP64-pipe bound.  Algorithmic work per
+    # (sample, beam pixel) evaluation = the FP64 flops of the reference
+    # algorithm executed directly on this GPU (ncu: dadd + dmul + 2 dfma on
+    # the direct-evaluation path); peak = FP64 FMA throughput measured now.
     peaks, peak_src = measured_peaks()
-    itemsize = 8
-    bytes_per_launch = (B * (4 * 11 + 8 * 3 * 2) + S * 16 + map_footprint_bytes(wl, itemsize))
-    achieved = bytes_per_launch / (kernel_ms / 1e3) / 1e9
-    traffic = profiled_traffic(args.mode)
-    roofline = {"bound": "hbm", "achieved": round(achieved, 1), "peak": peaks["hbm_gbs"],
-                "unit": "GB/s", "frac": round(achieved / peaks["hbm_gbs"], 4),
-                "traffic": traffic, "peak_source": peak_src,
-                "algorithmic_bytes_per_launch": int(bytes_per_launch),
-                "kernel": "gather_accum_kernel", "kernel_ms": round(kernel_ms, 3),
-                "note": "compute-bound on the FP64 pipe; bytes are the compulsory DRAM traffic"}
+    evals = float(B) * S
+    flops_per_eval = FLOPS_PER_EVAL[args.mode]
+    fp64_peak = fp64_peak_tflops()
+    achieved = evals * flops_per_eval / (kernel_ms / 1e3) / 1e12
+    bytes_per_launch = (B * (4 * 11 + 8 * 3 * 2) + S * 16 + map_footprint_bytes(wl, 8))
+    hbm_achieved = bytes_per_launch / (kernel_ms / 1e3) / 1e9
+    roofline = {"bound": "fp64", "achieved": round(achieved, 3), "peak": round(fp64_peak, 3),
+                "unit": "TFLOP/s", "frac": round(achieved / fp64_peak, 4),
+                "traffic": profiled_traffic(args.mode),
+                "peak_source": "measured now (todgpu_fp64_probe: 8 independent FMA chains/thread)",
+                "algorithmic_flops_per_eval": flops_per_eval,
+                "evals_per_launch": int(evals), "kernel": "gather_accum_kernel",
+                "kernel_ms": round(kernel_ms, 3),
+                "hbm": {"achieved": round(hbm_achieved, 2), "peak": peaks["hbm_gbs"], "unit": "GB/s",
+                        "frac": round(hbm_achieved / peaks["hbm_gbs"], 5),
+                        "algorithmic_bytes_per_launch": int(bytes_per_launch),
+                        "peak_source": peak_src}}
 
     result = {"value": value, "ms_per_step": total_ms / args.steps, "roofline": roofline,
               "clocks": clk, "gpu_launches": args.steps}

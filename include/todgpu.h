@@ -42,6 +42,8 @@ extern "C" {
 /* Element types. */
 #define TODGPU_F32 0
 #define TODGPU_F64 1
+/* params_dtype: pointing given as angles, rotation derived on the device. */
+#define TODGPU_ANGLES 2
 
 /*
  * Arguments of one fused gather/accumulate call: one beam entry over a batch
@@ -57,6 +59,13 @@ extern "C" {
  *   device rounds its float64 atan2 to float32 instead (Q/U may then differ
  *   from the reference by ~1e-7 relative on some samples).
  * params_dtype = TODGPU_F64: all float64, bore_phi ignored (precision form).
+ * params_dtype = TODGPU_ANGLES: the seven parameter arrays are not read;
+ *   theta, phi, psi (B,) (angles_dtype float32 or float64) and the beam centre
+ *   (center_phi, center_theta) give the pointing, and every CTA derives the
+ *   sample's rotation in float64 on the device (the steps of
+ *   precompute_rotation_vector_batch, tod_rotations.py:219-303, and
+ *   _rotation_params, :306-333, with psi_b - beta as the roll, gridint.py:281,
+ *   and no float32 rounding); vec_orig is then float64 (S, 3).
  *
  * map: planar (C, map_stride) of map_dtype, RING order, map_stride >= 12*nside^2.
  * beam_vals: (S,) float32.  err_count: optional device uint64 counter that
@@ -91,6 +100,13 @@ typedef struct todgpu_gather_args {
   int32_t reserved;
   const void *ring_table;/* optional: table built by todgpu_ring_table_build for this
                             nside; NULL evaluates ring data and spin-2 angles directly */
+  const void *theta;     /* (B,) boresight colatitude (TODGPU_ANGLES) */
+  const void *phi;       /* (B,) boresight longitude */
+  const void *psi;       /* (B,) polarisation angle psi_b */
+  int32_t angles_dtype;  /* TODGPU_F32 or TODGPU_F64 */
+  int32_t reserved2;
+  double center_phi;     /* beam centre longitude = ra[centre] */
+  double center_theta;   /* beam centre colatitude = pi/2 - dec[centre] */
 } todgpu_gather_args;
 
 /* Fused rotate -> HEALPix stencil -> spin-2 -> gather -> accumulate.

@@ -18,7 +18,7 @@ ABI_VERSION = 1
 OK = 0
 EINVAL, ENSIDE, ESHAPE, EDTYPE, ECUDA, EABI = -1, -2, -3, -4, -5, -6
 BILINEAR, NEAREST = 0, 1
-F32, F64 = 0, 1
+F32, F64, ANGLES = 0, 1, 2
 FLAG_NO_TABLES = 1
 
 _i32 = ctypes.c_int32
@@ -57,6 +57,13 @@ class GatherArgs(ctypes.Structure):
         ("flags", _i32),
         ("reserved", _i32),
         ("ring_table", _p),
+        ("theta", _p),
+        ("phi", _p),
+        ("psi", _p),
+        ("angles_dtype", _i32),
+        ("reserved2", _i32),
+        ("center_phi", ctypes.c_double),
+        ("center_theta", ctypes.c_double),
     ]
 
 

@@ -69,6 +69,12 @@ struct KArgs {
   const void* cos_p;
   const void* sin_p;
   const float* bore_phi;
+  const void* theta;         // pointing angles (angles mode)
+  const void* phi;
+  const void* psi;
+  int angles_f32;            // angles are float32 (else float64)
+  double cvx, cvy, cvz;      // beam-centre unit vector (angles mode)
+  double cnx, cny, cnz;      // its local north
   const float* beam;
   const void* map;
   long long map_stride;
@@ -77,10 +83,69 @@ struct KArgs {
   unsigned long long* err;
 };
 
-template <bool P64>
+// Pointing modes of the per-sample rotation.
+constexpr int kParamsRef32 = 0;  // reference float32 parameter arrays
+constexpr int kParamsF64 = 1;    // float64 parameter arrays
+constexpr int kAngles = 2;       // (theta, phi, psi) + beam centre, derived on the device
+
+template <int PM>
+__device__ __forceinline__ double angle_at(const KArgs& a, const void* p, long long b) {
+  return a.angles_f32 ? (double)static_cast<const float*>(p)[b] : static_cast<const double*>(p)[b];
+}
+
+// Rotation of sample b from its pointing angles, in float64: the Rodrigues
+// vector taking the beam centre c to the boresight t and the polarisation
+// offset beta (tod_rotations.py:219-303), then the parameters of
+// tod_rotations.py:306-333 without any float32 rounding.
+__device__ __forceinline__ SampleRot rot_from_angles(const KArgs& a, long long b) {
+  const double th = angle_at<kAngles>(a, a.theta, b), ph = angle_at<kAngles>(a, a.phi, b);
+  const double ps = angle_at<kAngles>(a, a.psi, b);
+  double st, ct, sp, cp;
+  sincos(th, &st, &ct);
+  sincos(ph, &sp, &cp);
+  const double tx = st * cp, ty = st * sp, tz = ct;    // boresight
+  const double nx = cp * ct, ny = sp * ct, nz = -st;   // its north
+  const double ex = -sp, ey = cp;                      // its east
+  double kx = a.cvy * tz - a.cvz * ty;
+  double ky = a.cvz * tx - a.cvx * tz;
+  double kz = a.cvx * ty - a.cvy * tx;
+  const double kn = sqrt((kx * kx + ky * ky) + kz * kz);
+  if (kn > 1e-10) {
+    kx /= kn;
+    ky /= kn;
+    kz /= kn;
+  } else {
+    kx = ky = kz = 0.0;
+  }
+  const double ang = acos(clamp1(a.cvx * tx + a.cvy * ty + a.cvz * tz));
+  double sa, ca;
+  sincos(ang, &sa, &ca);
+  const double dkn = kx * a.cnx + ky * a.cny + kz * a.cnz;
+  const double oma = 1.0 - ca;
+  const double wx = a.cnx * ca + (ky * a.cnz - kz * a.cny) * sa + kx * dkn * oma;
+  const double wy = a.cny * ca + (kz * a.cnx - kx * a.cnz) * sa + ky * dkn * oma;
+  const double wz = a.cnz * ca + (kx * a.cny - ky * a.cnx) * sa + kz * dkn * oma;
+  double beta = atan2(wx * ex + wy * ey + wz * 0.0, wx * nx + wy * ny + wz * nz);
+  if (beta < 0.0) beta += kTwoPi;
+  SampleRot r;
+  r.kx = kx;
+  r.ky = ky;
+  r.kz = kz;
+  r.ca = ca;
+  r.sa = sa;
+  r.px = tx;
+  r.py = ty;
+  r.pz = tz;
+  sincos(ps - beta, &r.sp, &r.cp);
+  return r;
+}
+
+template <int PM>
 __device__ __forceinline__ SampleRot load_rot(const KArgs& a, long long b) {
   SampleRot r;
-  if constexpr (P64) {
+  if constexpr (PM == kAngles) {
+    r = rot_from_angles(a, b);
+  } else if constexpr (PM == kParamsF64) {
     const double* ax = static_cast<const double*>(a.axes) + 3 * b;
     const double* pt = static_cast<const double*>(a.pts) + 3 * b;
     r.kx = ax[0];
@@ -118,10 +183,14 @@ __device__ __forceinline__ SampleRot load_rot(const KArgs& a, long long b) {
 // Boresight (z, sin theta, phi) of the spin-2 angle.  Float32 parameters use
 // the reference's typing: sin theta from a float32 square, phi from float32
 // atan2 (host libm value when provided).
-template <bool P64>
-__device__ __forceinline__ void load_boresight(const KArgs& a, long long b, double& z, double& sth,
-                                               double& phi) {
-  if constexpr (P64) {
+template <int PM>
+__device__ __forceinline__ void load_boresight(const KArgs& a, const SampleRot& rot, long long b, double& z,
+                                               double& sth, double& phi) {
+  if constexpr (PM == kAngles) {
+    z = clamp1(rot.pz);
+    sth = sqrt(max0(1.0 - rot.pz * rot.pz));
+    phi = atan2(rot.py, rot.px);
+  } else if constexpr (PM == kParamsF64) {
     const double* pt = static_cast<const double*>(a.pts) + 3 * b;
     z = clamp1(pt[2]);
     sth = sqrt(max0(1.0 - pt[2] * pt[2]));
@@ -140,11 +209,12 @@ __device__ __forceinline__ void load_boresight(const KArgs& a, long long b, doub
   if (phi < 0.0) phi += kTwoPi;
 }
 
-// Rotated beam pixel s of the sample.
-template <bool P64>
+// Rotated beam pixel s of the sample (float64 beam vectors in the float64
+// and angles modes).
+template <int PM>
 __device__ __forceinline__ void rotate_pixel(const KArgs& a, const SampleRot& r, long long s, double& vx,
                                              double& vy, double& vz) {
-  if constexpr (P64) {
+  if constexpr (PM != kParamsRef32) {
     const double* v = static_cast<const double*>(a.vec) + 3 * s;
     rot_f64(r, __ldg(v), __ldg(v + 1), __ldg(v + 2), vx, vy, vz);
   } else {
@@ -253,12 +323,12 @@ __device__ __forceinline__ void spin2_lookup(const Spin2Tab& w, const double2* t
 
 // Beam centre direction (normalised mean of the beam vectors) and the
 // largest angle between it and any beam vector; block-wide, once per CTA.
-template <bool P64, int NT>
+template <int PM, int NT>
 __device__ void beam_extent(const KArgs& a, double* s_red, double& cx, double& cy, double& cz, double& radius) {
   constexpr int NW = NT / 32;
   double sx = 0.0, sy = 0.0, sz = 0.0;
   for (long long s = threadIdx.x; s < a.S; s += NT) {
-    if constexpr (P64) {
+    if constexpr (PM != kParamsRef32) {
       const double* v = static_cast<const double*>(a.vec) + 3 * s;
       sx += v[0];
       sy += v[1];
@@ -299,7 +369,7 @@ __device__ void beam_extent(const KArgs& a, double* s_red, double& cx, double& c
   double mind = 1.0;
   for (long long s = threadIdx.x; s < a.S; s += NT) {
     double vx, vy, vz;
-    if constexpr (P64) {
+    if constexpr (PM != kParamsRef32) {
       const double* v = static_cast<const double*>(a.vec) + 3 * s;
       vx = v[0];
       vy = v[1];
@@ -328,7 +398,7 @@ __device__ void beam_extent(const KArgs& a, double* s_red, double& cx, double& c
 // One beam pixel's contribution, accumulated into acc[0..3]: generic path
 // (64-bit indices, any ring provider, any component layout).  Used without a
 // ring table and for non-finite rotated vectors.
-template <int MODE, bool HAS_QU, typename MapT, bool P64, class Rings>
+template <int MODE, bool HAS_QU, typename MapT, class Rings>
 __device__ __noinline__ void eval_generic(const KArgs& a, const Bore& bo, const Rings& rings, const Spin2Tab& w,
                                           const double2* tab, double vx, double vy, double vz, double phi_w,
                                           float bvf, double acc[4], unsigned long long& nerr) {
@@ -657,7 +727,7 @@ __device__ __forceinline__ void flush_sample(const KArgs& a, const double* s_red
 // Main kernel.  With a ring table: ring data come from it and, when the
 // entry carries Q and U, each sample's footprint gets a spin-2 table in
 // shared memory.  Without one: everything is evaluated directly.
-template <int MODE, bool HAS_QU, typename MapT, bool P64, int LAYOUT, int NT, int MINB>
+template <int MODE, bool HAS_QU, typename MapT, int PM, int LAYOUT, int NT, int MINB>
 __global__ void __launch_bounds__(NT, MINB) gather_accum_kernel(const KArgs a) {
   constexpr int NW = NT / 32;
   extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -673,7 +743,7 @@ __global__ void __launch_bounds__(NT, MINB) gather_accum_kernel(const KArgs a) {
   bool use_tab = false;
   if (rt != nullptr && HAS_QU) {
     double rbeam;
-    beam_extent<P64, NT>(a, s_red, cx, cy, cz, rbeam);
+    beam_extent<PM, NT>(a, s_red, cx, cy, cz, rbeam);
     // every stencil neighbour centre lies within 1.7/nside rad of the query
     // (one ring spacing plus one pixel width; the opposite pair around a pole
     // within twice the colatitude of ring 1); 3/nside leaves margin, plus
@@ -692,9 +762,9 @@ __global__ void __launch_bounds__(NT, MINB) gather_accum_kernel(const KArgs a) {
   unsigned long long nerr = 0;
   long long prev = -1;
   for (long long b = blockIdx.x; b < a.B; b += gridDim.x) {
-    const SampleRot rot = load_rot<P64>(a, b);
+    const SampleRot rot = load_rot<PM>(a, b);
     Bore bo{0.0, 0.0, 0.0};
-    if (HAS_QU) load_boresight<P64>(a, b, bo.z, bo.sth, bo.phi);
+    if (HAS_QU) load_boresight<PM>(a, rot, b, bo.z, bo.sth, bo.phi);
     __syncthreads();  // previous sample is done with the table and its partial sums
     if (prev >= 0 && threadIdx.x == 0) flush_sample<NW>(a, s_red, prev);
     if (use_tab) {
@@ -766,17 +836,17 @@ __global__ void __launch_bounds__(NT, MINB) gather_accum_kernel(const KArgs a) {
     double acc[4] = {0.0, 0.0, 0.0, 0.0};
     for (long long s = threadIdx.x; s < a.S; s += NT) {
       double vx, vy, vz;
-      rotate_pixel<P64>(a, rot, s, vx, vy, vz);
+      rotate_pixel<PM>(a, rot, s, vx, vy, vz);
       const float bvf = __ldg(a.beam + s);
       double phi_w = atan2(vy, vx);
       if (phi_w < 0.0) phi_w += kTwoPi;
       if (fast && isfinite(vx) && isfinite(vy) && isfinite(vz)) {
         eval_fast<MODE, HAS_QU, MapT, LAYOUT>(a, bo, rt, w, tab, vx, vy, vz, phi_w, bvf, acc);
       } else if (rt != nullptr) {
-        eval_generic<MODE, HAS_QU, MapT, P64>(a, bo, TableRings{rt}, w, tab, vx, vy, vz, phi_w, bvf, acc, nerr);
+        eval_generic<MODE, HAS_QU, MapT>(a, bo, TableRings{rt}, w, tab, vx, vy, vz, phi_w, bvf, acc, nerr);
       } else {
-        eval_generic<MODE, HAS_QU, MapT, P64>(a, bo, DirectRings{a.nside, a.npix}, w, tab, vx, vy, vz, phi_w, bvf,
-                                              acc, nerr);
+        eval_generic<MODE, HAS_QU, MapT>(a, bo, DirectRings{a.nside, a.npix}, w, tab, vx, vy, vz, phi_w, bvf,
+                                         acc, nerr);
       }
     }
 #pragma unroll
@@ -875,15 +945,15 @@ __global__ void ring_prefix_kernel(long long nside, RingRec* t) {
 // Small parity kernels (one thread per element).
 // ---------------------------------------------------------------------------
 
-template <bool P64>
+template <int PM>
 __global__ void stencil_kernel(const KArgs a, long long* pix, double* wgt) {
   const long long BS = a.B * a.S;
   for (long long n = blockIdx.x * (long long)blockDim.x + threadIdx.x; n < BS;
        n += (long long)gridDim.x * blockDim.x) {
     const long long b = n / a.S, s = n - b * a.S;
-    const SampleRot rot = load_rot<P64>(a, b);
+    const SampleRot rot = load_rot<PM>(a, b);
     double vx, vy, vz;
-    if constexpr (P64) {
+    if constexpr (PM != kParamsRef32) {
       const double* v = static_cast<const double*>(a.vec) + 3 * s;
       rot_f64(rot, v[0], v[1], v[2], vx, vy, vz);
     } else {
@@ -1038,11 +1108,11 @@ static __device__ __align__(256) RingRec g_static_ring_table[4 * kStaticMaxNside
 
 // Header of a table built from the beam on the device: the footprint reach the
 // gather kernel derives from the same beam (same code, plus a hair of margin).
-template <bool P64>
+template <int PM>
 __global__ void __launch_bounds__(kNTStatic) static_reach_kernel(const KArgs a, RingRec* t) {
   __shared__ double s_red[(kNTStatic / 32) * 4];
   double cx, cy, cz, rbeam;
-  beam_extent<P64, kNTStatic>(a, s_red, cx, cy, cz, rbeam);
+  beam_extent<PM, kNTStatic>(a, s_red, cx, cy, cz, rbeam);
   if (threadIdx.x == 0) {
     RingRec h;
     h.z = (double)a.nside;
@@ -1108,9 +1178,9 @@ constexpr size_t kTabHeaderBytes = (sizeof(Spin2Tab) + 15) & ~size_t(15);
 constexpr int kNT = TODGPU_CTA_THREADS;  // threads per CTA
 constexpr int kMinB = TODGPU_CTA_MINB;   // CTAs per SM the register budget is sized for
 
-template <int MODE, bool HAS_QU, typename MapT, bool P64, int LAYOUT>
+template <int MODE, bool HAS_QU, typename MapT, int PM, int LAYOUT>
 static int launch_gather(KArgs k, cudaStream_t stream) {
-  auto kern = gather_accum_kernel<MODE, HAS_QU, MapT, P64, LAYOUT, kNT, kMinB>;
+  auto kern = gather_accum_kernel<MODE, HAS_QU, MapT, PM, LAYOUT, kNT, kMinB>;
   static LaunchInfo info;
   static std::mutex mu;
   const int tab_cap = (HAS_QU && k.ring_table != nullptr) ? kTabCapDefault : 0;
@@ -1137,21 +1207,23 @@ static int launch_gather(KArgs k, cudaStream_t stream) {
   return TODGPU_OK;
 }
 
-template <int MODE, typename MapT, bool P64>
+template <int MODE, typename MapT, int PM>
 static int dispatch_qu(const KArgs& k, bool has_qu, cudaStream_t s) {
-  if (has_qu && k.C == 3 && k.c_q == 1 && k.c_u == 2) return launch_gather<MODE, true, MapT, P64, kLayoutIQU>(k, s);
-  return has_qu ? launch_gather<MODE, true, MapT, P64, kLayoutGeneric>(k, s)
-                : launch_gather<MODE, false, MapT, P64, kLayoutGeneric>(k, s);
+  if (has_qu && k.C == 3 && k.c_q == 1 && k.c_u == 2) return launch_gather<MODE, true, MapT, PM, kLayoutIQU>(k, s);
+  return has_qu ? launch_gather<MODE, true, MapT, PM, kLayoutGeneric>(k, s)
+                : launch_gather<MODE, false, MapT, PM, kLayoutGeneric>(k, s);
 }
 
 template <int MODE>
 static int dispatch_types(const KArgs& k, bool has_qu, int map_dtype, int params_dtype, cudaStream_t s) {
   if (map_dtype == TODGPU_F32) {
-    return params_dtype == TODGPU_F32 ? dispatch_qu<MODE, float, false>(k, has_qu, s)
-                                      : dispatch_qu<MODE, float, true>(k, has_qu, s);
+    if (params_dtype == TODGPU_F32) return dispatch_qu<MODE, float, kParamsRef32>(k, has_qu, s);
+    if (params_dtype == TODGPU_F64) return dispatch_qu<MODE, float, kParamsF64>(k, has_qu, s);
+    return dispatch_qu<MODE, float, kAngles>(k, has_qu, s);
   }
-  return params_dtype == TODGPU_F32 ? dispatch_qu<MODE, double, false>(k, has_qu, s)
-                                    : dispatch_qu<MODE, double, true>(k, has_qu, s);
+  if (params_dtype == TODGPU_F32) return dispatch_qu<MODE, double, kParamsRef32>(k, has_qu, s);
+  if (params_dtype == TODGPU_F64) return dispatch_qu<MODE, double, kParamsF64>(k, has_qu, s);
+  return dispatch_qu<MODE, double, kAngles>(k, has_qu, s);
 }
 
 static int check_common(const todgpu_gather_args* a, bool need_map) {
@@ -1162,11 +1234,16 @@ static int check_common(const todgpu_gather_args* a, bool need_map) {
   if (a->nside < 1 || a->nside > kMaxNside)
     return fail(TODGPU_ENSIDE, "nside " + std::to_string(a->nside) + " outside [1, 16384]");
   if (a->B < 0 || a->S < 0) return fail(TODGPU_ESHAPE, "negative B or S");
-  if (a->params_dtype != TODGPU_F32 && a->params_dtype != TODGPU_F64)
-    return fail(TODGPU_EDTYPE, "params_dtype must be TODGPU_F32 or TODGPU_F64");
+  if (a->params_dtype != TODGPU_F32 && a->params_dtype != TODGPU_F64 && a->params_dtype != TODGPU_ANGLES)
+    return fail(TODGPU_EDTYPE, "params_dtype must be TODGPU_F32, TODGPU_F64 or TODGPU_ANGLES");
   if (a->B > 0 && a->S > 0) {
-    if (!a->vec_orig || !a->axes || !a->cos_a || !a->sin_a || !a->ax_pts || !a->cos_p || !a->sin_p)
+    if (a->params_dtype == TODGPU_ANGLES) {
+      if (!a->vec_orig || !a->theta || !a->phi || !a->psi) return fail(TODGPU_EINVAL, "NULL pointing array");
+      if (a->angles_dtype != TODGPU_F32 && a->angles_dtype != TODGPU_F64)
+        return fail(TODGPU_EDTYPE, "angles_dtype must be TODGPU_F32 or TODGPU_F64");
+    } else if (!a->vec_orig || !a->axes || !a->cos_a || !a->sin_a || !a->ax_pts || !a->cos_p || !a->sin_p) {
       return fail(TODGPU_EINVAL, "NULL parameter array");
+    }
   }
   if (need_map) {
     if (a->interp != TODGPU_BILINEAR && a->interp != TODGPU_NEAREST)
@@ -1203,6 +1280,21 @@ static KArgs make_kargs(const todgpu_gather_args* a) {
   k.cos_p = a->cos_p;
   k.sin_p = a->sin_p;
   k.bore_phi = a->bore_phi;
+  k.theta = a->theta;
+  k.phi = a->phi;
+  k.psi = a->psi;
+  k.angles_f32 = a->angles_dtype == TODGPU_F32 ? 1 : 0;
+  {
+    // beam centre and its north from (center_phi, center_theta)
+    const double st = std::sin(a->center_theta), ct = std::cos(a->center_theta);
+    const double sp = std::sin(a->center_phi), cp = std::cos(a->center_phi);
+    k.cvx = st * cp;
+    k.cvy = st * sp;
+    k.cvz = ct;
+    k.cnx = cp * ct;
+    k.cny = sp * ct;
+    k.cnz = -st;
+  }
   k.beam = a->beam_vals;
   k.map = a->map;
   k.map_stride = a->map_stride;
@@ -1272,9 +1364,9 @@ extern "C" int todgpu_gather_accum_static(const todgpu_gather_args* a, void* str
     // every call rebuilds the whole table (header, records, prefix sums) for
     // its own nside and beam, so nothing depends on earlier contents
     if (a->params_dtype == TODGPU_F32)
-      static_reach_kernel<false><<<1, kNTStatic, 0, s>>>(k, t);
+      static_reach_kernel<kParamsRef32><<<1, kNTStatic, 0, s>>>(k, t);
     else
-      static_reach_kernel<true><<<1, kNTStatic, 0, s>>>(k, t);
+      static_reach_kernel<kParamsF64><<<1, kNTStatic, 0, s>>>(k, t);
     ring_table_kernel<<<grid_for(4 * a->nside, 256), 256, 0, s>>>(a->nside, 0.0, t, true);
     ring_prefix_kernel<<<1, 1024, 0, s>>>(a->nside, t);
     cudaError_t e = cudaGetLastError();
@@ -1297,9 +1389,11 @@ extern "C" int todgpu_bilinear_stencils(const todgpu_gather_args* a, int64_t* pi
   cudaStream_t s = static_cast<cudaStream_t>(stream);
   const int g = grid_for(a->B * a->S, 256);
   if (a->params_dtype == TODGPU_F32)
-    stencil_kernel<false><<<g, 256, 0, s>>>(k, reinterpret_cast<long long*>(pix), wgt);
+    stencil_kernel<kParamsRef32><<<g, 256, 0, s>>>(k, reinterpret_cast<long long*>(pix), wgt);
+  else if (a->params_dtype == TODGPU_F64)
+    stencil_kernel<kParamsF64><<<g, 256, 0, s>>>(k, reinterpret_cast<long long*>(pix), wgt);
   else
-    stencil_kernel<true><<<g, 256, 0, s>>>(k, reinterpret_cast<long long*>(pix), wgt);
+    stencil_kernel<kAngles><<<g, 256, 0, s>>>(k, reinterpret_cast<long long*>(pix), wgt);
   cudaError_t e = cudaGetLastError();
   return e == cudaSuccess ? TODGPU_OK : cuda_fail(e, "stencil_kernel launch");
 }

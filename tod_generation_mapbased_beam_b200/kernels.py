@@ -214,3 +214,71 @@ def bilinear_stencils(vec_orig, axes, cos_a, sin_a, ax_pts, cos_p, sin_p, nside,
     _native.check(_native.lib().todgpu_bilinear_stencils(ctypes.byref(a), pix.data_ptr(),
                                                          wgt.data_ptr(), stream_handle()))
     return pix, wgt
+
+
+def beam_center_angles(ra, dec, center_idx=None):
+    """(phi_c, theta_c) of the beam centre: the grid centre by default, as
+    tod_rotations.py:251-261 chooses it."""
+    ra = np.asarray(ra)
+    dec = np.asarray(dec)
+    if center_idx is None:
+        center_idx = (ra.shape[0] // 2, ra.shape[1] // 2)
+    return float(ra[center_idx]), float(np.pi / 2 - dec[center_idx])
+
+
+def gather_accum_angles(interp, vec_orig, theta, phi, psi, center_phi, center_theta, nside,
+                        mp_stacked, beam_vals, tod, c_q=-1, c_u=-1, err_count=None, flags=0,
+                        static_table=False):
+    """One fused launch with the pointing given as angles: every CTA derives
+    the sample's rotation on the device in float64 from (theta, phi, psi) and
+    the beam centre (no float32 parameter rounding).  ``tod`` must be a float64
+    (C, B) CUDA tensor; it is accumulated in place.  ``theta, phi, psi`` may be
+    float32 or float64 (a float32 scan is widened exactly on the device)."""
+    require_cuda()
+    vec = to_device(vec_orig, np.float64).reshape(-1, 3)
+    S = vec.shape[0]
+    adt = dtype_of(theta)
+    adt = np.float32 if adt == np.dtype(np.float32) else np.float64
+    th = to_device(theta, adt).reshape(-1)
+    ph = to_device(phi, adt).reshape(-1)
+    ps = to_device(psi, adt).reshape(-1)
+    B = th.shape[0]
+    if ph.shape[0] != B or ps.shape[0] != B:
+        raise ValueError("theta, phi and psi must have the same length")
+    beam = to_device(beam_vals, np.float32, (S,))
+    mp = _map_tensor(mp_stacked)
+    C = mp.shape[0]
+    if not (is_tensor(tod) and tod.is_cuda and tod.dtype == torch.float64 and tod.dim() == 2
+            and tod.stride(1) == 1 and tuple(tod.shape) == (C, B)):
+        raise ValueError(f"tod must be a float64 CUDA tensor of shape {(C, B)} with unit stride")
+    a = _native.GatherArgs()
+    a.abi_version = _native.ABI_VERSION
+    a.interp = interp
+    a.nside = int(nside)
+    a.B = B
+    a.S = S
+    a.C = C
+    a.c_q = int(c_q)
+    a.c_u = int(c_u)
+    a.params_dtype = _native.ANGLES
+    a.map_dtype = _native.F32 if mp.dtype == torch.float32 else _native.F64
+    a.vec_orig = vec.data_ptr()
+    a.theta, a.phi, a.psi = th.data_ptr(), ph.data_ptr(), ps.data_ptr()
+    a.angles_dtype = _native.F32 if adt == np.float32 else _native.F64
+    a.center_phi = float(center_phi)
+    a.center_theta = float(center_theta)
+    a.beam_vals = beam.data_ptr()
+    a.map = mp.data_ptr()
+    a.map_stride = mp.stride(0)
+    a.tod = tod.data_ptr()
+    a.tod_stride = tod.stride(0)
+    a.err_count = ptr(err_count)
+    a.flags = int(flags)
+    lib = _native.lib()
+    if static_table:
+        _native.check(lib.todgpu_gather_accum_static(ctypes.byref(a), stream_handle()))
+        return tod
+    if not flags & _native.FLAG_NO_TABLES and B > 0 and S > 0:
+        a.ring_table = ring_table(nside, beam_reach(vec, nside), vec.device).data_ptr()
+    _native.check(lib.todgpu_gather_accum(ctypes.byref(a), stream_handle()))
+    return tod

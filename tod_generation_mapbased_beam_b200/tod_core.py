@@ -29,7 +29,7 @@ import torch
 
 from . import _native
 from ._device import is_tensor, require_cuda
-from .kernels import boresight_phi_host, gather_accum
+from .kernels import beam_center_angles, boresight_phi_host, gather_accum, gather_accum_angles
 from .tod_rotations import _rotation_params, precompute_rotation_vector_batch  # noqa: F401
 
 _INTERP = {"bilinear": _native.BILINEAR, "nearest": _native.NEAREST}
@@ -124,6 +124,41 @@ def beam_tod_batch(nside, mp, data, rot_vecs, phi_b, theta_b, psis_b, interp_mod
     tod = torch.zeros((C, B), dtype=torch.float64, device=mpd.device)
     gather_accum(_INTERP[interp_mode], vec, *params, nside, mpd, bv, B, S, tod, c_q, c_u,
                  bore_phi=bore_phi if bore_phi is not None else np.zeros(B, np.float32))
+    if return_device:
+        return tod
+    host = tod.to(torch.float32).cpu().numpy()
+    return {comp: host[i] for i, comp in enumerate(comp_indices)}
+
+
+def beam_tod_angles(nside, data, theta_b, phi_b, psi_b, interp_mode="bilinear", *,
+                    center=None, mp=None, return_device=False):
+    """Device-pointing variant of :func:`beam_tod_batch` for one beam entry.
+
+    Takes the scan angles themselves -- ``theta_b, phi_b, psi_b`` (B,), float32
+    as the reference driver reads them (gridint.py:277-279) or float64 -- and
+    derives each sample's rotation on the GPU in float64 (the steps of
+    ``precompute_rotation_vector_batch`` and ``_rotation_params`` with the roll
+    psi_b - beta, gridint.py:280-281), without the reference's float32
+    parameter rounding.  ``center`` is (phi_c, theta_c) of the beam centre;
+    by default the centre of ``data['ra'], data['dec']``.
+    Returns ``{comp: float32 (B,)}`` or the float64 (C, B) CUDA tensor."""
+    B = int(np.asarray(theta_b).shape[0]) if not is_tensor(theta_b) else int(theta_b.shape[0])
+    comp_indices = list(data["comp_indices"])
+    C = len(comp_indices)
+    c_q, c_u = component_slots(comp_indices)
+    if interp_mode not in ("nearest", "bilinear"):
+        raise ValueError(
+            f"interp_mode {interp_mode!r} not available on main branch; "
+            "switch to the 'gaussian' or 'bicubic' branch")
+    require_cuda()
+    if center is None:
+        center = beam_center_angles(data["ra"], data["dec"])
+    vec = _cache.get(data["vec_orig"], torch.float64)
+    bv = _cache.get(data["beam_vals"], torch.float32)
+    mpd = stacked_map(data, mp)
+    tod = torch.zeros((C, B), dtype=torch.float64, device=mpd.device)
+    gather_accum_angles(_INTERP[interp_mode], vec, theta_b, phi_b, psi_b, center[0], center[1], nside,
+                        mpd, bv, tod, c_q, c_u)
     if return_device:
         return tod
     host = tod.to(torch.float32).cpu().numpy()

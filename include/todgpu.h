@@ -44,6 +44,13 @@ extern "C" {
 #define TODGPU_F64 1
 /* params_dtype: pointing given as angles, rotation derived on the device. */
 #define TODGPU_ANGLES 2
+/* map_dtype of the precision form: one record of 4 components per pixel,
+ * float32 (16 B) or bfloat16 (8 B), made by todgpu_pack_map.  With a packed
+ * map the spin-2 angles are kept in float32 and the sum over beam pixels is
+ * float32 with Kahan compensation; rotation, pixel choice and weights stay
+ * float64. */
+#define TODGPU_PACKED_F32 2
+#define TODGPU_PACKED_BF16 3
 
 /*
  * Arguments of one fused gather/accumulate call: one beam entry over a batch
@@ -67,7 +74,8 @@ extern "C" {
  *   _rotation_params, :306-333, with psi_b - beta as the roll, gridint.py:281,
  *   and no float32 rounding); vec_orig is then float64 (S, 3).
  *
- * map: planar (C, map_stride) of map_dtype, RING order, map_stride >= 12*nside^2.
+ * map: planar (C, map_stride) of map_dtype, RING order, map_stride >= 12*nside^2;
+ *   or, for TODGPU_PACKED_*, N records of 4 components (map_stride ignored).
  * beam_vals: (S,) float32.  err_count: optional device uint64 counter that
  * receives the number of (b, s) terms skipped because a stencil pixel fell
  * outside the map (non-finite pointing); pass NULL to ignore.
@@ -179,6 +187,14 @@ int todgpu_boresight_phi_host(const float *ax_pts, int64_t B, float *out, int32_
  * cache spin-2 angles per sample (tod_bilinear.py:151-199). */
 size_t todgpu_ring_table_bytes(int64_t nside);
 int todgpu_ring_table_build(int64_t nside, double reach, void *table, size_t bytes, void *stream);
+
+/* Pack a planar (C, N) float32/float64 map (row stride `stride` elements) into
+ * N records of 4 components for the precision form: packed_dtype
+ * TODGPU_PACKED_F32 (16 B/pixel, `out` 16-byte aligned) or TODGPU_PACKED_BF16
+ * (8 B/pixel, round to nearest even).  No counterpart in the reference, which
+ * reads planar mp_stacked (gridint.py:447-450). */
+int todgpu_pack_map(const void *planar, int32_t planar_dtype, int64_t C, int64_t N, int64_t stride,
+                    int32_t packed_dtype, void *out, void *stream);
 
 /* FP64 pipe throughput probe (measurement helper; no counterpart in the
  * reference): launches `blocks` CTAs of 256 threads running `iters` rounds of

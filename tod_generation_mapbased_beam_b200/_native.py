@@ -19,6 +19,7 @@ OK = 0
 EINVAL, ENSIDE, ESHAPE, EDTYPE, ECUDA, EABI = -1, -2, -3, -4, -5, -6
 BILINEAR, NEAREST = 0, 1
 F32, F64, ANGLES = 0, 1, 2
+PACKED_F32, PACKED_BF16 = 2, 3
 FLAG_NO_TABLES = 1
 
 _i32 = ctypes.c_int32
@@ -100,6 +101,8 @@ def _declare(lib):
     lib.todgpu_ring_table_bytes.restype = ctypes.c_size_t
     lib.todgpu_ring_table_build.argtypes = [_i64, ctypes.c_double, _p, ctypes.c_size_t, _p]
     lib.todgpu_ring_table_build.restype = ctypes.c_int
+    lib.todgpu_pack_map.argtypes = [_p, _i32, _i64, _i64, _i64, _i32, _p, _p]
+    lib.todgpu_pack_map.restype = ctypes.c_int
     lib.todgpu_fp64_probe.argtypes = [_i64, _i32, _p, ctypes.POINTER(ctypes.c_double), _p]
     lib.todgpu_fp64_probe.restype = ctypes.c_int
     lib.todgpu_abi_version.argtypes = []
@@ -148,6 +151,7 @@ def exported_symbols():
         "todgpu_boresight_phi_host",
         "todgpu_ring_table_bytes",
         "todgpu_ring_table_build",
+        "todgpu_pack_map",
         "todgpu_fp64_probe",
         "todgpu_abi_version",
         "todgpu_last_error_string",

@@ -24,6 +24,7 @@
 //
 // Compiled with -fmad=false: the pixel decisions and the FP64 accumulation
 // reproduce the reference's uncontracted arithmetic.
+#include <cuda_bf16.h>
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -33,6 +34,7 @@
 #include <mutex>
 #include <string>
 #include <thread>
+#include <type_traits>
 #include <vector>
 
 #include "healpix_ring.cuh"
@@ -223,21 +225,108 @@ __device__ __forceinline__ void rotate_pixel(const KArgs& a, const SampleRot& r,
   }
 }
 
+struct PackF32;
+struct PackBF16;
+template <typename MapT>
+__device__ __forceinline__ float4 load_rec(const KArgs& a, long long p);
+__device__ __forceinline__ float rec_at(const float4& r, int c);
+
 template <typename MapT>
 __device__ __forceinline__ double map_at(const KArgs& a, int c, long long p) {
-  return (double)__ldg(static_cast<const MapT*>(a.map) + (long long)c * a.map_stride + p);
+  if constexpr (std::is_same<MapT, PackF32>::value || std::is_same<MapT, PackBF16>::value)
+    return (double)rec_at(load_rec<MapT>(a, p), c);
+  else
+    return (double)__ldg(static_cast<const MapT*>(a.map) + (long long)c * a.map_stride + p);
 }
 
 // mp[c, p] * bv with the nearest kernel's typing (tod_nearest.py:146, :158):
 // a float32 map element times the float32 weight is a float32 product.
 template <typename MapT>
 __device__ __forceinline__ double map_x_beam(const KArgs& a, int c, long long p, float bv) {
-  const MapT m = __ldg(static_cast<const MapT*>(a.map) + (long long)c * a.map_stride + p);
-  if constexpr (sizeof(MapT) == 4)
-    return (double)(m * bv);
-  else
-    return m * (double)bv;
+  if constexpr (std::is_same<MapT, PackF32>::value || std::is_same<MapT, PackBF16>::value) {
+    return (double)(rec_at(load_rec<MapT>(a, p), c) * bv);
+  } else {
+    const MapT m = __ldg(static_cast<const MapT*>(a.map) + (long long)c * a.map_stride + p);
+    if constexpr (sizeof(MapT) == 4)
+      return (double)(m * bv);
+    else
+      return m * (double)bv;
+  }
 }
+
+// ---------------------------------------------------------------------------
+// Map element types.  Planar float/double maps are the reference's
+// mp_stacked (C, N); the precision form packs a pixel's components into one
+// record: PackF32 = 4 x float32 (16 B), PackBF16 = 4 x bfloat16 (8 B).  The
+// precision form also keeps cos 2d / sin 2d in float32 and accumulates in
+// float32 with Kahan compensation; pixel decisions and weights stay float64.
+// ---------------------------------------------------------------------------
+
+struct PackF32 {};
+struct PackBF16 {};
+
+template <typename MapT>
+struct MapTraits {
+  static constexpr bool packed = false;
+  using Tab = double2;
+};
+template <>
+struct MapTraits<PackF32> {
+  static constexpr bool packed = true;
+  using Tab = float2;
+};
+template <>
+struct MapTraits<PackBF16> {
+  static constexpr bool packed = true;
+  using Tab = float2;
+};
+
+__device__ __forceinline__ float bf16_lo(unsigned v) { return __uint_as_float(v << 16); }
+__device__ __forceinline__ float bf16_hi(unsigned v) { return __uint_as_float(v & 0xffff0000u); }
+
+template <typename MapT>
+__device__ __forceinline__ float4 load_rec(const KArgs& a, long long p) {
+  if constexpr (std::is_same<MapT, PackF32>::value) {
+    return __ldg(static_cast<const float4*>(a.map) + p);
+  } else {
+    const uint2 r = __ldg(static_cast<const uint2*>(a.map) + p);
+    return make_float4(bf16_lo(r.x), bf16_hi(r.x), bf16_lo(r.y), bf16_hi(r.y));
+  }
+}
+
+__device__ __forceinline__ float rec_at(const float4& r, int c) {
+  return c == 0 ? r.x : (c == 1 ? r.y : (c == 2 ? r.z : r.w));
+}
+
+template <typename TabT>
+__device__ __forceinline__ TabT make_tab(double c, double s);
+template <>
+__device__ __forceinline__ double2 make_tab<double2>(double c, double s) {
+  return make_double2(c, s);
+}
+template <>
+__device__ __forceinline__ float2 make_tab<float2>(double c, double s) {
+  return make_float2((float)c, (float)s);
+}
+
+// Per-thread accumulators: float64 (parity path) or float32 with Kahan
+// compensation (precision form).
+struct Acc64 {
+  double v[4] = {0.0, 0.0, 0.0, 0.0};
+  __device__ __forceinline__ void add(int c, double x) { v[c] += x; }
+  __device__ __forceinline__ double total(int c) const { return v[c]; }
+};
+struct AccKahan {
+  float s[4] = {0.f, 0.f, 0.f, 0.f};
+  float e[4] = {0.f, 0.f, 0.f, 0.f};  // running compensation (minus the lost low bits)
+  __device__ __forceinline__ void add(int c, float x) {
+    const float y = x - e[c];
+    const float t = s[c] + y;
+    e[c] = (t - s[c]) - y;
+    s[c] = t;
+  }
+  __device__ __forceinline__ double total(int c) const { return (double)s[c] - (double)e[c]; }
+};
 
 __device__ __forceinline__ double warp_sum(double v) {
 #pragma unroll
@@ -298,7 +387,8 @@ struct Bore {
   double z, sth, phi;
 };
 
-__device__ __forceinline__ void spin2_lookup(const Spin2Tab& w, const double2* tab, long long ring, long long ip,
+template <typename TabT>
+__device__ __forceinline__ void spin2_lookup(const Spin2Tab& w, const TabT* tab, long long ring, long long ip,
                                              long long n, double zn, double phin, const Bore& bo, double& c2d,
                                              double& s2d) {
   // ip is the pixel's in-ring index and n its ring's length; the spill case
@@ -310,9 +400,9 @@ __device__ __forceinline__ void spin2_lookup(const Spin2Tab& w, const double2* t
     if (j >= 0 && j < w.cap[r]) {
       const long long slot = w.off[r] + j;
       if (slot < w.total) {
-        const double2 v = tab[slot];
-        c2d = v.x;
-        s2d = v.y;
+        const TabT v = tab[slot];
+        c2d = (double)v.x;
+        s2d = (double)v.y;
         return;
       }
     }
@@ -398,10 +488,10 @@ __device__ void beam_extent(const KArgs& a, double* s_red, double& cx, double& c
 // One beam pixel's contribution, accumulated into acc[0..3]: generic path
 // (64-bit indices, any ring provider, any component layout).  Used without a
 // ring table and for non-finite rotated vectors.
-template <int MODE, bool HAS_QU, typename MapT, class Rings>
+template <int MODE, bool HAS_QU, typename MapT, class Rings, typename TabT, class Acc>
 __device__ __noinline__ void eval_generic(const KArgs& a, const Bore& bo, const Rings& rings, const Spin2Tab& w,
-                                          const double2* tab, double vx, double vy, double vz, double phi_w,
-                                          float bvf, double acc[4], unsigned long long& nerr) {
+                                          const TabT* tab, double vx, double vy, double vz, double phi_w,
+                                          float bvf, Acc& acc, unsigned long long& nerr) {
   const double bv = (double)bvf;
   if constexpr (MODE == TODGPU_BILINEAR) {
     const double z = clamp1(vz);
@@ -437,11 +527,11 @@ __device__ __noinline__ void eval_generic(const KArgs& a, const Bore& bo, const 
     }
     for (int c = 0; c < a.C; ++c) {
       if (HAS_QU && c == a.c_q)
-        acc[c] = fma(tq, bv, acc[c]);
+        acc.add(c, tq * bv);
       else if (HAS_QU && c == a.c_u)
-        acc[c] = fma(tu, bv, acc[c]);
+        acc.add(c, tu * bv);
       else
-        acc[c] = fma(to[c], bv, acc[c]);
+        acc.add(c, to[c] * bv);
     }
   } else {
     const double sin_th = sqrt(max0(vx * vx + vy * vy));
@@ -457,14 +547,14 @@ __device__ __noinline__ void eval_generic(const KArgs& a, const Bore& bo, const 
       const double uv = map_at<MapT>(a, a.c_u, nb.pix);
       for (int c = 0; c < a.C; ++c) {
         if (c == a.c_q)
-          acc[c] = fma(fma(qv, c2d, uv * s2d), bv, acc[c]);
+          acc.add(c, fma(qv, c2d, uv * s2d) * bv);
         else if (c == a.c_u)
-          acc[c] = fma(fma(uv, c2d, -qv * s2d), bv, acc[c]);
+          acc.add(c, fma(uv, c2d, -qv * s2d) * bv);
         else
-          acc[c] += map_x_beam<MapT>(a, c, nb.pix, bvf);
+          acc.add(c, map_x_beam<MapT>(a, c, nb.pix, bvf));
       }
     } else {
-      for (int c = 0; c < a.C; ++c) acc[c] += map_x_beam<MapT>(a, c, nb.pix, bvf);
+      for (int c = 0; c < a.C; ++c) acc.add(c, map_x_beam<MapT>(a, c, nb.pix, bvf));
     }
   }
 }
@@ -570,7 +660,8 @@ __device__ __forceinline__ void stencil_fast(int nside, double z, double phi_w, 
 }
 
 // Table lookup with 32-bit indices (ip == n is the spill case: direct).
-__device__ __forceinline__ void spin2_fast(const Spin2Tab& w, const double2* tab, int ring, int ip, int n, double zn,
+template <typename TabT>
+__device__ __forceinline__ void spin2_fast(const Spin2Tab& w, const TabT* tab, int ring, int ip, int n, double zn,
                                            double phin, const Bore& bo, double& c2d, double& s2d) {
   const unsigned r = (unsigned)(ring - w.ir_lo32);
   if (r < (unsigned)w.nr && (unsigned)ip < (unsigned)n) {
@@ -578,9 +669,9 @@ __device__ __forceinline__ void spin2_fast(const Spin2Tab& w, const double2* tab
     j += (j >> 31) & n;
     const int slot = w.off[r] + j;
     if ((unsigned)j < (unsigned)w.cap[r] && slot < w.total) {
-      const double2 v = tab[slot];
-      c2d = v.x;
-      s2d = v.y;
+      const TabT v = tab[slot];
+      c2d = (double)v.x;
+      s2d = (double)v.y;
       return;
     }
   }
@@ -613,44 +704,80 @@ __device__ __forceinline__ double map_x_beam_i(const KArgs& a, int c, int p, flo
     return m * (double)bv;
 }
 
-template <int MODE, bool HAS_QU, typename MapT, int LAYOUT>
+template <int MODE, bool HAS_QU, typename MapT, int LAYOUT, typename TabT, class Acc>
 __device__ __forceinline__ void eval_fast(const KArgs& a, const Bore& bo, const RingRec* rt, const Spin2Tab& w,
-                                          const double2* tab, double vx, double vy, double vz, double phi_w,
-                                          float bvf, double acc[4]) {
+                                          const TabT* tab, double vx, double vy, double vz, double phi_w,
+                                          float bvf, Acc& acc) {
+  constexpr bool kPacked = MapTraits<MapT>::packed;
   const Chan<LAYOUT> ch(a);
   const int nside = (int)a.nside;
   const double bv = (double)bvf;
   if constexpr (MODE == TODGPU_BILINEAR) {
     const double z = clamp1(vz);
-    double tq = 0.0, tu = 0.0, to[4] = {0.0, 0.0, 0.0, 0.0};
-    stencil_fast(nside, z, phi_w, rt, [&](int k, int p, double wk, int ring, int ip, int n, double zn, double phin) {
-      if constexpr (HAS_QU) {
-        double c2, s2;
-        spin2_fast(w, tab, ring, ip, n, zn, phin, bo, c2, s2);
-        const double q = map_i<MapT>(a, ch.q, p);
-        const double u = map_i<MapT>(a, ch.u, p);
-        const double vq = wk * fma(q, c2, u * s2);
-        const double vu = wk * fma(u, c2, -q * s2);
-        tq = (k == 0) ? vq : tq + vq;
-        tu = (k == 0) ? vu : tu + vu;
-      }
+    if constexpr (kPacked) {
+      // precision form: one record per neighbour, float32 mixing
+      float tq = 0.f, tu = 0.f, to[4] = {0.f, 0.f, 0.f, 0.f};
+      stencil_fast(nside, z, phi_w, rt, [&](int k, int p, double wk, int ring, int ip, int n, double zn, double phin) {
+        const float4 rec = load_rec<MapT>(a, p);
+        const float wf = (float)wk;
+        if constexpr (HAS_QU) {
+          double c2, s2;
+          spin2_fast(w, tab, ring, ip, n, zn, phin, bo, c2, s2);
+          const float c2f = (float)c2, s2f = (float)s2;
+          const float q = rec_at(rec, ch.q), u = rec_at(rec, ch.u);
+          const float vq = wf * fmaf(q, c2f, u * s2f);
+          const float vu = wf * fmaf(u, c2f, -q * s2f);
+          tq = (k == 0) ? vq : tq + vq;
+          tu = (k == 0) ? vu : tu + vu;
+        }
+#pragma unroll
+        for (int c = 0; c < 4; ++c) {
+          if (c >= ch.C) break;
+          if (HAS_QU && (c == ch.q || c == ch.u)) continue;
+          to[c] = (k == 0) ? wf * rec_at(rec, c) : fmaf(wf, rec_at(rec, c), to[c]);
+        }
+      });
 #pragma unroll
       for (int c = 0; c < 4; ++c) {
         if (c >= ch.C) break;
-        if (HAS_QU && (c == ch.q || c == ch.u)) continue;
-        const double m = map_i<MapT>(a, c, p);
-        to[c] = (k == 0) ? wk * m : fma(wk, m, to[c]);
+        if (HAS_QU && c == ch.q)
+          acc.add(c, tq * bvf);
+        else if (HAS_QU && c == ch.u)
+          acc.add(c, tu * bvf);
+        else
+          acc.add(c, to[c] * bvf);
       }
-    });
+    } else {
+      double tq = 0.0, tu = 0.0, to[4] = {0.0, 0.0, 0.0, 0.0};
+      stencil_fast(nside, z, phi_w, rt, [&](int k, int p, double wk, int ring, int ip, int n, double zn, double phin) {
+        if constexpr (HAS_QU) {
+          double c2, s2;
+          spin2_fast(w, tab, ring, ip, n, zn, phin, bo, c2, s2);
+          const double q = map_i<MapT>(a, ch.q, p);
+          const double u = map_i<MapT>(a, ch.u, p);
+          const double vq = wk * fma(q, c2, u * s2);
+          const double vu = wk * fma(u, c2, -q * s2);
+          tq = (k == 0) ? vq : tq + vq;
+          tu = (k == 0) ? vu : tu + vu;
+        }
 #pragma unroll
-    for (int c = 0; c < 4; ++c) {
-      if (c >= ch.C) break;
-      if (HAS_QU && c == ch.q)
-        acc[c] = fma(tq, bv, acc[c]);
-      else if (HAS_QU && c == ch.u)
-        acc[c] = fma(tu, bv, acc[c]);
-      else
-        acc[c] = fma(to[c], bv, acc[c]);
+        for (int c = 0; c < 4; ++c) {
+          if (c >= ch.C) break;
+          if (HAS_QU && (c == ch.q || c == ch.u)) continue;
+          const double m = map_i<MapT>(a, c, p);
+          to[c] = (k == 0) ? wk * m : fma(wk, m, to[c]);
+        }
+      });
+#pragma unroll
+      for (int c = 0; c < 4; ++c) {
+        if (c >= ch.C) break;
+        if (HAS_QU && c == ch.q)
+          acc.add(c, tq * bv);
+        else if (HAS_QU && c == ch.u)
+          acc.add(c, tu * bv);
+        else
+          acc.add(c, to[c] * bv);
+      }
     }
   } else {
     // nearest: unclamped z; |z| > 1 makes the reference's ring_above NaN-based
@@ -689,7 +816,26 @@ __device__ __forceinline__ void eval_fast(const KArgs& a, const Bore& bo, const 
         }
       }
     }
-    if constexpr (HAS_QU) {
+    if constexpr (kPacked) {
+      const float4 rec = load_rec<MapT>(a, best_pix);
+      float c2f = 1.f, s2f = 0.f;
+      if constexpr (HAS_QU) {
+        double c2d, s2d;
+        spin2_fast(w, tab, best_ring, best_ip, best_n, best_zc, best_phic, bo, c2d, s2d);
+        c2f = (float)c2d;
+        s2f = (float)s2d;
+      }
+#pragma unroll
+      for (int c = 0; c < 4; ++c) {
+        if (c >= ch.C) break;
+        if (HAS_QU && c == ch.q)
+          acc.add(c, fmaf(rec_at(rec, ch.q), c2f, rec_at(rec, ch.u) * s2f) * bvf);
+        else if (HAS_QU && c == ch.u)
+          acc.add(c, fmaf(rec_at(rec, ch.u), c2f, -rec_at(rec, ch.q) * s2f) * bvf);
+        else
+          acc.add(c, rec_at(rec, c) * bvf);
+      }
+    } else if constexpr (HAS_QU) {
       double c2d, s2d;
       spin2_fast(w, tab, best_ring, best_ip, best_n, best_zc, best_phic, bo, c2d, s2d);
       const double qv = map_i<MapT>(a, ch.q, best_pix);
@@ -698,17 +844,17 @@ __device__ __forceinline__ void eval_fast(const KArgs& a, const Bore& bo, const 
       for (int c = 0; c < 4; ++c) {
         if (c >= ch.C) break;
         if (c == ch.q)
-          acc[c] = fma(fma(qv, c2d, uv * s2d), bv, acc[c]);
+          acc.add(c, fma(qv, c2d, uv * s2d) * bv);
         else if (c == ch.u)
-          acc[c] = fma(fma(uv, c2d, -qv * s2d), bv, acc[c]);
+          acc.add(c, fma(uv, c2d, -qv * s2d) * bv);
         else
-          acc[c] += map_x_beam_i<MapT>(a, c, best_pix, bvf);
+          acc.add(c, map_x_beam_i<MapT>(a, c, best_pix, bvf));
       }
     } else {
 #pragma unroll
       for (int c = 0; c < 4; ++c) {
         if (c >= ch.C) break;
-        acc[c] += map_x_beam_i<MapT>(a, c, best_pix, bvf);
+        acc.add(c, map_x_beam_i<MapT>(a, c, best_pix, bvf));
       }
     }
   }
@@ -732,7 +878,9 @@ __global__ void __launch_bounds__(NT, MINB) gather_accum_kernel(const KArgs a) {
   constexpr int NW = NT / 32;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   Spin2Tab& w = *reinterpret_cast<Spin2Tab*>(smem_raw);
-  double2* tab = reinterpret_cast<double2*>(smem_raw + ((sizeof(Spin2Tab) + 15) & ~size_t(15)));
+  using TabT = typename MapTraits<MapT>::Tab;
+  using Acc = typename std::conditional<MapTraits<MapT>::packed, AccKahan, Acc64>::type;
+  TabT* tab = reinterpret_cast<TabT*>(smem_raw + ((sizeof(Spin2Tab) + 15) & ~size_t(15)));
   __shared__ double s_red[NW * 4];
 
   constexpr int kSetupThreads = 64;  // threads that derive a sample's footprint window
@@ -828,12 +976,12 @@ __global__ void __launch_bounds__(NT, MINB) gather_accum_kernel(const KArgs a) {
         const double phin = __ldg(&r->phi0) + (double)ip * __ldg(&r->dphi);
         double c2, s2;
         spin2_c2s2(__ldg(&r->z), __ldg(&r->sth), phin, bo.z, bo.sth, bo.phi, c2, s2);
-        tab[e] = make_double2(c2, s2);
+        tab[e] = make_tab<TabT>(c2, s2);
       }
     }
     __syncthreads();
 
-    double acc[4] = {0.0, 0.0, 0.0, 0.0};
+    Acc acc;
     for (long long s = threadIdx.x; s < a.S; s += NT) {
       double vx, vy, vz;
       rotate_pixel<PM>(a, rot, s, vx, vy, vz);
@@ -852,7 +1000,7 @@ __global__ void __launch_bounds__(NT, MINB) gather_accum_kernel(const KArgs a) {
 #pragma unroll
     for (int c = 0; c < 4; ++c) {
       if (c >= a.C) break;
-      const double v = warp_sum(acc[c]);
+      const double v = warp_sum(acc.total(c));
       if (lane == 0) s_red[warp * 4 + c] = v;
     }
     prev = b;
@@ -1128,6 +1276,26 @@ __global__ void __launch_bounds__(kNTStatic) static_reach_kernel(const KArgs a, 
   }
 }
 
+// Planar (C, N) float/double map -> one record per pixel of 4 components
+// (float32 or bfloat16, round to nearest even; missing components are 0).
+template <typename SrcT, bool BF16>
+__global__ void pack_map_kernel(const SrcT* src, int C, long long N, long long stride, void* out) {
+  for (long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x; p < N; p += (long long)gridDim.x * blockDim.x) {
+    float v[4] = {0.f, 0.f, 0.f, 0.f};
+    for (int c = 0; c < C; ++c) v[c] = (float)src[(long long)c * stride + p];
+    if constexpr (BF16) {
+      __nv_bfloat162 lo = __floats2bfloat162_rn(v[0], v[1]);
+      __nv_bfloat162 hi = __floats2bfloat162_rn(v[2], v[3]);
+      uint2 r;
+      r.x = *reinterpret_cast<unsigned*>(&lo);
+      r.y = *reinterpret_cast<unsigned*>(&hi);
+      static_cast<uint2*>(out)[p] = r;
+    } else {
+      static_cast<float4*>(out)[p] = make_float4(v[0], v[1], v[2], v[3]);
+    }
+  }
+}
+
 // FP64 pipe throughput probe: 8 independent FMA chains per thread, so the
 // pipe, not latency, bounds it.  flops = 2 * 8 * iters per thread.
 __global__ void fp64_probe_kernel(int iters, double seed, double* out) {
@@ -1183,9 +1351,12 @@ static int launch_gather(KArgs k, cudaStream_t stream) {
   auto kern = gather_accum_kernel<MODE, HAS_QU, MapT, PM, LAYOUT, kNT, kMinB>;
   static LaunchInfo info;
   static std::mutex mu;
-  const int tab_cap = (HAS_QU && k.ring_table != nullptr) ? kTabCapDefault : 0;
-  const size_t smem = kTabHeaderBytes + sizeof(double2) * (size_t)tab_cap;
-  const size_t smem_max = kTabHeaderBytes + sizeof(double2) * (size_t)kTabCapDefault;
+  using TabT = typename MapTraits<MapT>::Tab;
+  // 32 KiB of spin-2 table: 2048 float64 pairs or 4096 float32 pairs
+  constexpr int kCap = (int)(kTabCapDefault * sizeof(double2) / sizeof(TabT));
+  const int tab_cap = (HAS_QU && k.ring_table != nullptr) ? kCap : 0;
+  const size_t smem = kTabHeaderBytes + sizeof(TabT) * (size_t)tab_cap;
+  const size_t smem_max = kTabHeaderBytes + sizeof(TabT) * (size_t)kCap;
   {
     std::lock_guard<std::mutex> lock(mu);
     if (!info.configured) {
@@ -1216,6 +1387,16 @@ static int dispatch_qu(const KArgs& k, bool has_qu, cudaStream_t s) {
 
 template <int MODE>
 static int dispatch_types(const KArgs& k, bool has_qu, int map_dtype, int params_dtype, cudaStream_t s) {
+  if (map_dtype == TODGPU_PACKED_F32) {
+    if (params_dtype == TODGPU_F32) return dispatch_qu<MODE, PackF32, kParamsRef32>(k, has_qu, s);
+    if (params_dtype == TODGPU_F64) return dispatch_qu<MODE, PackF32, kParamsF64>(k, has_qu, s);
+    return dispatch_qu<MODE, PackF32, kAngles>(k, has_qu, s);
+  }
+  if (map_dtype == TODGPU_PACKED_BF16) {
+    if (params_dtype == TODGPU_F32) return dispatch_qu<MODE, PackBF16, kParamsRef32>(k, has_qu, s);
+    if (params_dtype == TODGPU_F64) return dispatch_qu<MODE, PackBF16, kParamsF64>(k, has_qu, s);
+    return dispatch_qu<MODE, PackBF16, kAngles>(k, has_qu, s);
+  }
   if (map_dtype == TODGPU_F32) {
     if (params_dtype == TODGPU_F32) return dispatch_qu<MODE, float, kParamsRef32>(k, has_qu, s);
     if (params_dtype == TODGPU_F64) return dispatch_qu<MODE, float, kParamsF64>(k, has_qu, s);
@@ -1252,10 +1433,13 @@ static int check_common(const todgpu_gather_args* a, bool need_map) {
     if (a->c_q < -1 || a->c_q >= a->C || a->c_u < -1 || a->c_u >= a->C)
       return fail(TODGPU_ESHAPE, "c_q/c_u must be -1 or a component index");
     if (a->c_q >= 0 && a->c_q == a->c_u) return fail(TODGPU_ESHAPE, "c_q == c_u");
-    if (a->map_dtype != TODGPU_F32 && a->map_dtype != TODGPU_F64)
-      return fail(TODGPU_EDTYPE, "map_dtype must be TODGPU_F32 or TODGPU_F64");
+    const bool packed = a->map_dtype == TODGPU_PACKED_F32 || a->map_dtype == TODGPU_PACKED_BF16;
+    if (a->map_dtype != TODGPU_F32 && a->map_dtype != TODGPU_F64 && !packed)
+      return fail(TODGPU_EDTYPE, "map_dtype must be TODGPU_F32, TODGPU_F64, TODGPU_PACKED_F32 or TODGPU_PACKED_BF16");
     const long long npix = 12 * a->nside * a->nside;
-    if (a->map_stride < npix) return fail(TODGPU_ESHAPE, "map_stride < 12*nside^2");
+    if (!packed && a->map_stride < npix) return fail(TODGPU_ESHAPE, "map_stride < 12*nside^2");
+    if (packed && ((uintptr_t)a->map & (a->map_dtype == TODGPU_PACKED_F32 ? 15 : 7)) != 0)
+      return fail(TODGPU_EINVAL, "packed map must be aligned to its record size");
     if (a->tod_stride < a->B) return fail(TODGPU_ESHAPE, "tod_stride < B");
     if (a->B > 0 && a->S > 0 && (!a->map || !a->tod || !a->beam_vals))
       return fail(TODGPU_EINVAL, "NULL map, tod or beam_vals");
@@ -1497,6 +1681,34 @@ extern "C" int todgpu_fp64_probe(int64_t blocks, int32_t iters, double* sink, do
   if (e != cudaSuccess) return cuda_fail(e, "fp64_probe_kernel launch");
   *flops = 2.0 * 8.0 * (double)iters * 256.0 * (double)blocks;
   return TODGPU_OK;
+}
+
+extern "C" int todgpu_pack_map(const void* planar, int32_t planar_dtype, int64_t C, int64_t N, int64_t stride,
+                               int32_t packed_dtype, void* out, void* stream) {
+  if (!planar || !out) return fail(TODGPU_EINVAL, "NULL pointer");
+  if (C < 1 || C > 4 || N < 0 || stride < N) return fail(TODGPU_ESHAPE, "bad map shape");
+  if (planar_dtype != TODGPU_F32 && planar_dtype != TODGPU_F64) return fail(TODGPU_EDTYPE, "planar dtype");
+  if (packed_dtype != TODGPU_PACKED_F32 && packed_dtype != TODGPU_PACKED_BF16)
+    return fail(TODGPU_EDTYPE, "packed dtype");
+  if (((uintptr_t)out & (packed_dtype == TODGPU_PACKED_F32 ? 15 : 7)) != 0)
+    return fail(TODGPU_EINVAL, "packed map must be aligned to its record size");
+  if (N == 0) return TODGPU_OK;
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  const int g = grid_for(N, 256);
+  const bool bf = packed_dtype == TODGPU_PACKED_BF16;
+  if (planar_dtype == TODGPU_F32) {
+    if (bf)
+      pack_map_kernel<float, true><<<g, 256, 0, s>>>(static_cast<const float*>(planar), (int)C, N, stride, out);
+    else
+      pack_map_kernel<float, false><<<g, 256, 0, s>>>(static_cast<const float*>(planar), (int)C, N, stride, out);
+  } else {
+    if (bf)
+      pack_map_kernel<double, true><<<g, 256, 0, s>>>(static_cast<const double*>(planar), (int)C, N, stride, out);
+    else
+      pack_map_kernel<double, false><<<g, 256, 0, s>>>(static_cast<const double*>(planar), (int)C, N, stride, out);
+  }
+  cudaError_t e = cudaGetLastError();
+  return e == cudaSuccess ? TODGPU_OK : cuda_fail(e, "pack_map_kernel launch");
 }
 
 extern "C" int todgpu_abi_version(void) { return TODGPU_ABI_VERSION; }

@@ -99,6 +99,21 @@ def ring_table(nside, reach, device=None):
     return t
 
 
+def _set_map(a, mp):
+    if isinstance(mp, PackedMap):
+        a.map_dtype = mp.map_dtype
+        a.map = mp.data.data_ptr()
+        a.map_stride = mp.npix
+    else:
+        a.map_dtype = _native.F32 if mp.dtype == torch.float32 else _native.F64
+        a.map = mp.data_ptr()
+        a.map_stride = mp.stride(0)
+
+
+def _ncomp(mp):
+    return mp.C if isinstance(mp, PackedMap) else mp.shape[0]
+
+
 def make_args(interp, nside, B, S, C, c_q, c_u, params, pdt, bore_phi, beam, mp, tod,
               err=None, flags=0, table=None):
     a = _native.GatherArgs()
@@ -111,12 +126,10 @@ def make_args(interp, nside, B, S, C, c_q, c_u, params, pdt, bore_phi, beam, mp,
     a.c_q = int(c_q)
     a.c_u = int(c_u)
     a.params_dtype = _native.F32 if pdt == np.float32 else _native.F64
-    a.map_dtype = _native.F32 if mp.dtype == torch.float32 else _native.F64
+    _set_map(a, mp)
     (a.vec_orig, a.axes, a.cos_a, a.sin_a, a.ax_pts, a.cos_p, a.sin_p) = [ptr(t) for t in params]
     a.bore_phi = ptr(bore_phi)
     a.beam_vals = ptr(beam)
-    a.map = ptr(mp)
-    a.map_stride = mp.stride(0)
     a.tod = ptr(tod)
     a.tod_stride = tod.stride(0)
     a.err_count = ptr(err)
@@ -125,7 +138,46 @@ def make_args(interp, nside, B, S, C, c_q, c_u, params, pdt, bore_phi, beam, mp,
     return a
 
 
+class PackedMap:
+    """A map in the precision form's layout: one record of 4 components per
+    pixel (float32, 16 B, or bfloat16, 8 B), built by :func:`pack_map`."""
+
+    def __init__(self, data: torch.Tensor, C: int, kind: str):
+        self.data = data
+        self.C = int(C)
+        self.kind = kind  # "f32" or "bf16"
+
+    @property
+    def map_dtype(self):
+        return _native.PACKED_F32 if self.kind == "f32" else _native.PACKED_BF16
+
+    @property
+    def npix(self):
+        return self.data.shape[0]
+
+
+def pack_map(mp_stacked, kind="f32"):
+    """Pack a planar (C, N) map (numpy or torch, float32/float64, C <= 4) into
+    the precision form's per-pixel records on the GPU (todgpu_pack_map)."""
+    if kind not in ("f32", "bf16"):
+        raise ValueError("kind must be 'f32' or 'bf16'")
+    mp = _map_tensor(mp_stacked)
+    C, N = mp.shape
+    if C > 4:
+        raise ValueError("at most 4 components per record")
+    if kind == "f32":
+        out = torch.empty((N, 4), dtype=torch.float32, device=mp.device)
+    else:
+        out = torch.empty((N, 4), dtype=torch.bfloat16, device=mp.device)
+    _native.check(_native.lib().todgpu_pack_map(
+        mp.data_ptr(), _native.F32 if mp.dtype == torch.float32 else _native.F64, C, N, mp.stride(0),
+        _native.PACKED_F32 if kind == "f32" else _native.PACKED_BF16, out.data_ptr(), stream_handle()))
+    return PackedMap(out, C, kind)
+
+
 def _map_tensor(mp_stacked):
+    if isinstance(mp_stacked, PackedMap):
+        return mp_stacked
     dt = dtype_of(mp_stacked)
     if dt not in (np.dtype(np.float32), np.dtype(np.float64)):
         raise TypeError(f"mp_stacked must be float32 or float64, got {dt}")
@@ -157,7 +209,7 @@ def gather_accum(interp, vec_orig, axes, cos_a, sin_a, ax_pts, cos_p, sin_p, nsi
         raise TypeError("beam_vals must be float32 (the reference casts beam weights to float32)")
     beam = to_device(beam_vals, np.float32, (S,))
     mp = _map_tensor(mp_stacked)
-    C = mp.shape[0]
+    C = _ncomp(mp)
     if pdt == np.float32 and bore_phi is None and B > 0:
         bore_phi = boresight_phi_host(ax_pts if not is_tensor(ax_pts) else params[4])
     bphi = to_device(bore_phi, np.float32, (B,)) if (bore_phi is not None and pdt == np.float32) else None
@@ -247,7 +299,7 @@ def gather_accum_angles(interp, vec_orig, theta, phi, psi, center_phi, center_th
         raise ValueError("theta, phi and psi must have the same length")
     beam = to_device(beam_vals, np.float32, (S,))
     mp = _map_tensor(mp_stacked)
-    C = mp.shape[0]
+    C = _ncomp(mp)
     if not (is_tensor(tod) and tod.is_cuda and tod.dtype == torch.float64 and tod.dim() == 2
             and tod.stride(1) == 1 and tuple(tod.shape) == (C, B)):
         raise ValueError(f"tod must be a float64 CUDA tensor of shape {(C, B)} with unit stride")
@@ -261,15 +313,13 @@ def gather_accum_angles(interp, vec_orig, theta, phi, psi, center_phi, center_th
     a.c_q = int(c_q)
     a.c_u = int(c_u)
     a.params_dtype = _native.ANGLES
-    a.map_dtype = _native.F32 if mp.dtype == torch.float32 else _native.F64
+    _set_map(a, mp)
     a.vec_orig = vec.data_ptr()
     a.theta, a.phi, a.psi = th.data_ptr(), ph.data_ptr(), ps.data_ptr()
     a.angles_dtype = _native.F32 if adt == np.float32 else _native.F64
     a.center_phi = float(center_phi)
     a.center_theta = float(center_theta)
     a.beam_vals = beam.data_ptr()
-    a.map = mp.data_ptr()
-    a.map_stride = mp.stride(0)
     a.tod = tod.data_ptr()
     a.tod_stride = tod.stride(0)
     a.err_count = ptr(err_count)

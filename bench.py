@@ -49,8 +49,8 @@ METRIC = "TOD samples/s, 1 B200: FP64 plain vs mixed/learned-tail at fixed RMS e
 # FP64 flops per (sample, beam pixel) evaluation of the reference algorithm,
 # counted by ncu on the direct-evaluation path (TODGPU_FLAG_NO_TABLES) of the
 # config-2 workload: dadd + dmul + 2 * dfma per evaluation
-# (profiles/gather_accum_bilinear_config2.md).
-FLOPS_PER_EVAL = {"bilinear": 853.0, "nearest": 853.0}
+# (profiles/gather_accum_{bilinear,nearest}_config2.md).
+FLOPS_PER_EVAL = {"bilinear": 853.0, "nearest": 500.0}
 
 
 def parse_args():
@@ -63,6 +63,7 @@ def parse_args():
     p.add_argument("--samples", type=int, default=8_640_000)
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--no-mixed", action="store_true", help="skip the mixed-precision forms")
     p.add_argument("--no-tables", action="store_true",
                    help="evaluate ring data and spin-2 angles directly (A/B comparison)")
     p.add_argument("--cpu-seconds", type=float, default=10.0,
@@ -301,6 +302,28 @@ def profiled_traffic(mode):
     return None
 
 
+def mixed_error_uk(wl, mode, kind, tod, cargs, margs, lib, stream, n_sub=2000):
+    """RMS / max error [uK] of a mixed form against the FP64 oracle on the
+    first n_sub samples (the same float32 parameters, the float64 map)."""
+    import oracle
+    from tod_generation_mapbased_beam_b200 import _native
+    from tod_generation_mapbased_beam_b200 import tod_rotations as R
+
+    beam = wl["beam"]
+    sl = slice(0, n_sub)
+    params = R._rotation_params(wl["rot"][sl], wl["phi"][sl], wl["theta"][sl], wl["psis"][sl])
+    ref = np.zeros((3, n_sub))
+    fn = oracle.gather_accum_fused if mode == "bilinear" else oracle.gather_accum_nearest
+    fn(beam.vec_orig, *params, wl["nside"], wl["sky"], beam.beam_vals, n_sub, beam.S, ref, 1, 2,
+       nthreads=len(os.sched_getaffinity(0)))
+    tod.zero_()
+    _native.check(lib.todgpu_gather_accum(ctypes.byref(margs), stream.cuda_stream))
+    got = tod[:, :n_sub].cpu().numpy()
+    err = (got - ref) * 1e6
+    return {"rms_uK": float(np.sqrt(np.mean(err ** 2))), "max_uK": float(np.abs(err).max()),
+            "error_sample": f"{n_sub} samples vs FP64 oracle (same float32 parameters, float64 map)"}
+
+
 def run_ours(args, dist):
     import torch
 
@@ -387,6 +410,36 @@ def run_ours(args, dist):
 
     result = {"value": value, "ms_per_step": total_ms / args.steps, "roofline": roofline,
               "clocks": clk, "gpu_launches": args.steps}
+
+    # mixed precision forms on the same workload: packed float32 / bfloat16
+    # records, float32 spin-2 table, float32 Kahan sum, float64 decisions;
+    # error against the FP64 oracle on a bounded subset of samples
+    if not args.no_mixed:
+        from tod_generation_mapbased_beam_b200.kernels import pack_map
+
+        mixed = {}
+        for kind in ("f32", "bf16"):
+            pm = pack_map(sky, kind)
+            margs = make_args(interp, nside, B, S, 3, 1, 2, params, np.float32, bore, bv, pm, tod,
+                              table=table)
+            for _ in range(2):
+                _native.check(lib.todgpu_gather_accum(ctypes.byref(margs), stream.cuda_stream))
+            torch.cuda.synchronize()
+            m0 = torch.cuda.Event(enable_timing=True)
+            m1 = torch.cuda.Event(enable_timing=True)
+            m0.record(stream)
+            for _ in range(args.steps):
+                tod.zero_()
+                _native.check(lib.todgpu_gather_accum(ctypes.byref(margs), stream.cuda_stream))
+            m1.record(stream)
+            m1.synchronize()
+            mms = dist.max(m0.elapsed_time(m1) / args.steps)
+            entry = {"value": B * dist.world / (mms / 1e3), "ms_per_step": mms,
+                     "map": f"packed {kind} records ({16 if kind == 'f32' else 8} B/pixel)"}
+            if dist.rank == 0 and not args.no_cpu_baseline:
+                entry.update(mixed_error_uk(wl, args.mode, kind, tod, cargs, margs, lib, stream))
+            mixed[kind] = entry
+        result["mixed"] = mixed
 
     # end to end with host buffers: the day driver (host float32 scan in,
     # float64 (3, n) day TOD out, device pointing, pipelined copies), and the
@@ -483,7 +536,7 @@ def main():
                     scaling="weak", config=dict(config, S=S, parallelism=f"samples x{dist.world}"),
                     roofline=res["roofline"], gpu_launches=res["gpu_launches"],
                     clocks=res["clocks"])
-        for key in ("e2e", "e2e_drop_in"):
+        for key in ("e2e", "e2e_drop_in", "mixed"):
             if key in res:
                 line[key] = res[key]
         if "cpu_baseline" in res:

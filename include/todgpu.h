@@ -122,6 +122,19 @@ typedef struct todgpu_gather_args {
  * and tod_nearest._gather_accum_nearest_jit (tod_nearest.py:21-158). */
 int todgpu_gather_accum(const todgpu_gather_args *args, void *stream);
 
+/* Many jobs in one persistent launch: jobs[0 .. njobs) (a host array) are
+ * independent gathers -- typically one detector each, with its own beam
+ * (vec_orig, beam_vals, S), pointing (B samples) and output tod -- that share
+ * interp, nside, the component layout (C, c_q, c_u), params_dtype, map_dtype
+ * and flags.  Each job's samples are cut into tiles of `tile` samples; the
+ * tiles of all jobs are spread over the persistent grid in contiguous ranges.
+ * Results equal one todgpu_gather_accum call per job.  Up to 96 jobs travel
+ * in one launch's parameters; more are split over consecutive launches.
+ * Replaces a loop of beam_tod_batch calls over detectors (the reference has
+ * no batched-detector mode; gridint.py:284-296 loops over beam entries). */
+int todgpu_gather_accum_batched(const todgpu_gather_args *jobs, int32_t njobs, int64_t tile,
+                                void *stream);
+
 /* The same fused gather/accumulate as todgpu_gather_accum, for callers that
  * cannot allocate device memory themselves -- for example a host application
  * whose device memory is owned by another framework's allocator, or a foreign-

@@ -83,6 +83,8 @@ _lib = None
 def _declare(lib):
     lib.todgpu_gather_accum.argtypes = [ctypes.POINTER(GatherArgs), _p]
     lib.todgpu_gather_accum.restype = ctypes.c_int
+    lib.todgpu_gather_accum_batched.argtypes = [ctypes.POINTER(GatherArgs), _i32, _i64, _p]
+    lib.todgpu_gather_accum_batched.restype = ctypes.c_int
     lib.todgpu_gather_accum_static.argtypes = [ctypes.POINTER(GatherArgs), _p]
     lib.todgpu_gather_accum_static.restype = ctypes.c_int
     lib.todgpu_bilinear_stencils.argtypes = [ctypes.POINTER(GatherArgs), _p, _p, _p]
@@ -142,6 +144,7 @@ def exported_symbols():
     """Names of the C entry points declared in include/todgpu.h."""
     return [
         "todgpu_gather_accum",
+        "todgpu_gather_accum_batched",
         "todgpu_gather_accum_static",
         "todgpu_bilinear_stencils",
         "todgpu_get_interp_weights",

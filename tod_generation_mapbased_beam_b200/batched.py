@@ -1,0 +1,126 @@
+"""Batched detectors in one persistent launch (config 4 of the benchmark).
+
+:class:`DetectorBatch` holds, on the GPU, every detector's beam (vectors and
+weights), its scan angles and its (C, n) float64 output, and runs them all
+with one ``todgpu_gather_accum_batched`` launch -- the rotation of each sample
+derived on the device from its angles (FP64).  The launch is captured in a
+CUDA graph on first use and replayed afterwards (``graph=True``), and its
+tile size (samples per work tile) is chosen by :mod:`autotune` unless given.
+
+The reference has no batched mode: it loops over beam entries per batch
+(sample_based_tod_generation_gridint.py:284-296); one DetectorBatch run equals
+one gather per detector (tests/test_gpu_batched.py checks bit-identity).
+"""
+
+from __future__ import annotations
+
+import ctypes
+
+import numpy as np
+import torch
+
+from . import _native
+from ._device import require_cuda, stream_handle, to_device
+from .kernels import PackedMap, _map_tensor, _ncomp, _set_map, beam_reach, ring_table
+
+
+class DetectorBatch:
+    def __init__(self, nside, mp, detectors, comp_indices=(0, 1, 2), interp_mode="bilinear",
+                 tile=None, graph=True, tables=True):
+        require_cuda()
+        if interp_mode not in ("bilinear", "nearest"):
+            raise ValueError(f"interp_mode {interp_mode!r} not available on main branch; "
+                             "switch to the 'gaussian' or 'bicubic' branch")
+        self.nside = int(nside)
+        self.interp = _native.BILINEAR if interp_mode == "bilinear" else _native.NEAREST
+        self.map = _map_tensor(mp)
+        self.C = _ncomp(self.map)
+        comps = list(comp_indices)
+        if len(comps) != self.C:
+            raise ValueError("comp_indices must name one Stokes component per map component")
+        self.c_q = comps.index(1) if 1 in comps else -1
+        self.c_u = comps.index(2) if 2 in comps else -1
+        dev = torch.device("cuda", torch.cuda.current_device())
+        self.vec, self.beam, self.angles, self.out, self.centers = [], [], [], [], []
+        reach = 0.0
+        for d in detectors:
+            vec = to_device(d["vec_orig"], np.float64).reshape(-1, 3)
+            self.vec.append(vec)
+            self.beam.append(to_device(d["beam_vals"], np.float32).reshape(-1))
+            ang = [to_device(d[k], np.float32).reshape(-1) for k in ("theta", "phi", "psi")]
+            self.angles.append(ang)
+            self.out.append(torch.zeros((self.C, ang[0].shape[0]), dtype=torch.float64, device=dev))
+            self.centers.append(tuple(d.get("center", (0.0, 0.0))))
+            if vec.shape[0]:
+                reach = max(reach, beam_reach(vec, self.nside))
+        self.table = ring_table(self.nside, reach, dev) if (tables and reach > 0) else None
+        self.flags = 0 if tables else _native.FLAG_NO_TABLES
+        self._args = self._make_args()
+        self.tile = int(tile) if tile else None
+        self.use_graph = graph
+        self._graph = None
+
+    @property
+    def n_samples(self):
+        return sum(a[0].shape[0] for a in self.angles)
+
+    @property
+    def n_evals(self):
+        return sum(a[0].shape[0] * v.shape[0] for a, v in zip(self.angles, self.vec))
+
+    def _make_args(self):
+        arr = (_native.GatherArgs * len(self.vec))()
+        for j, (vec, bv, ang, out, cen) in enumerate(zip(self.vec, self.beam, self.angles, self.out,
+                                                          self.centers)):
+            a = arr[j]
+            a.abi_version = _native.ABI_VERSION
+            a.interp = self.interp
+            a.nside = self.nside
+            a.B = ang[0].shape[0]
+            a.S = vec.shape[0]
+            a.C = self.C
+            a.c_q, a.c_u = self.c_q, self.c_u
+            a.params_dtype = _native.ANGLES
+            _set_map(a, self.map)
+            a.vec_orig = vec.data_ptr()
+            a.theta, a.phi, a.psi = (t.data_ptr() for t in ang)
+            a.angles_dtype = _native.F32
+            a.center_phi, a.center_theta = cen
+            a.beam_vals = bv.data_ptr()
+            a.tod = out.data_ptr()
+            a.tod_stride = out.stride(0)
+            a.flags = self.flags
+            a.ring_table = None if self.table is None else self.table.data_ptr()
+        return arr
+
+    def launch(self, tile=None):
+        """Zero the outputs and launch once on the current stream (no graph)."""
+        for o in self.out:
+            o.zero_()
+        t = int(tile or self.tile or 256)
+        _native.check(_native.lib().todgpu_gather_accum_batched(self._args, len(self._args), t,
+                                                                stream_handle()))
+
+    def run(self):
+        """All detectors' (C, n) float64 outputs (CUDA tensors, in order)."""
+        if self.tile is None:
+            from .autotune import choose_tile
+
+            self.tile = choose_tile(self)
+        if not self.use_graph:
+            self.launch()
+            return self.out
+        if self._graph is None:
+            side = torch.cuda.Stream()
+            side.wait_stream(torch.cuda.current_stream())
+            with torch.cuda.stream(side):
+                self.launch()  # first launch configures the kernel outside the capture
+            torch.cuda.current_stream().wait_stream(side)
+            self._graph = torch.cuda.CUDAGraph()
+            with torch.cuda.graph(self._graph):
+                self.launch()
+        self._graph.replay()
+        return self.out
+
+    def release(self):
+        self._graph = None

@@ -28,8 +28,11 @@ INCLUDE = os.path.join(ROOT, "include")
 OUT_DIR = os.path.join(PKG, "_lib")
 LIB = os.path.join(OUT_DIR, "libtodgpu.so")
 
-SOURCES = ["tod_gather.cu"]
-HEADERS = ["healpix_ring.cuh"]
+# One translation unit per map element type (they instantiate the gather
+# kernels and compile in parallel) plus the C ABI.
+SOURCES = ["tod_api.cu", "gather_map_f64.cu", "gather_map_f32.cu", "gather_map_pf32.cu",
+           "gather_map_pbf16.cu"]
+HEADERS = ["healpix_ring.cuh", "gather_impl.cuh"]
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = ["-O3", "-std=c++17", "-lineinfo", "-fmad=false", "-Xcompiler", "-fPIC,-O2",
@@ -62,7 +65,7 @@ def build(force: bool = False, verbose: bool = False) -> str:
         return LIB
     os.makedirs(OUT_DIR, exist_ok=True)
     nvcc = nvcc_path()
-    objs = []
+    objs, procs = [], []
     for src in SOURCES:
         obj = os.path.join(OUT_DIR, os.path.splitext(src)[0] + ".o")
         cmd = [nvcc, *ARCH, *NVCC_FLAGS, "-I", INCLUDE, "-I", CSRC, "-c",
@@ -70,8 +73,11 @@ def build(force: bool = False, verbose: bool = False) -> str:
         if verbose:
             cmd.insert(1, "-Xptxas=-v")
             print(" ".join(cmd))
-        subprocess.run(cmd, check=True)
+        procs.append((src, subprocess.Popen(cmd)))
         objs.append(obj)
+    failed = [src for src, proc in procs if proc.wait() != 0]
+    if failed:
+        raise RuntimeError(f"nvcc failed for {failed}")
     tmp = LIB + ".tmp"
     cmd = [nvcc, *ARCH, "-shared", "-cudart", "static", "-o", tmp, *objs, "-lpthread"]
     if verbose:

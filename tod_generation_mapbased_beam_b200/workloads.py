@@ -127,3 +127,46 @@ def config2(n_samples=8_640_000, seed=1):
     theta, phi, psi = spin_scan(n_samples, 100.0)
     sky = white_sky(1024, seed)
     return dict(nside=1024, beam=beam, theta=theta, phi=phi, psi=psi, sky=sky)
+
+
+def rotate_beam(vec, pol_angle, offset_theta, offset_phi):
+    """Beam vectors centred on the beam-frame pole, turned by ``pol_angle``
+    about the pole and then moved so the pole lands at (offset_theta,
+    offset_phi): a detector whose beam sits off the boresight."""
+    v = np.asarray(vec, np.float64)
+    c, s = math.cos(pol_angle), math.sin(pol_angle)
+    v = np.stack([c * v[:, 0] - s * v[:, 1], s * v[:, 0] + c * v[:, 1], v[:, 2]], -1)
+    if offset_theta == 0.0:
+        return v
+    t = np.array([math.sin(offset_theta) * math.cos(offset_phi),
+                  math.sin(offset_theta) * math.sin(offset_phi), math.cos(offset_theta)])
+    k = np.cross([0.0, 0.0, 1.0], t)
+    k /= np.linalg.norm(k)
+    ca, sa = math.cos(offset_theta), math.sin(offset_theta)
+    return v * ca + np.cross(k, v) * sa + np.outer(v @ k, k) * (1 - ca)
+
+
+def config4(n_det=64, seed=4, n_min=1e5, n_max=9e6, nside=2048, beam_nside=2048, rate_hz=100.0):
+    """Batched form (config 4): detectors with their own beam (FWHM ~ U(25', 35'),
+    ellipticity ~ U(0, 0.1), polarisation angle ~ U(0, pi)), boresight offset
+    uniform in a 1 deg disc and a scan length ~ log-uniform in [n_min, n_max];
+    a float32 sky.  Returns (detectors, sky); each detector is a dict with
+    ``vec_orig`` (float64, offset beam), ``beam_vals``, ``theta, phi, psi``
+    (float32 scan of its own length and phase) and ``center`` (0, 0)."""
+    rng = np.random.default_rng(seed)
+    dets = []
+    for d in range(n_det):
+        fwhm = rng.uniform(25.0, 35.0)
+        ell = rng.uniform(0.0, 0.1)
+        pol = rng.uniform(0.0, math.pi)
+        r_off = math.radians(1.0) * math.sqrt(rng.uniform())
+        p_off = rng.uniform(0.0, 2 * math.pi)
+        n = int(round(math.exp(rng.uniform(math.log(n_min), math.log(n_max)))))
+        beam = pole_gaussian_beam(fwhm, beam_nside, 0.99, fwhm2_arcmin=fwhm * (1.0 - ell),
+                                  search_fwhm=1.5)
+        th, ph, ps = spin_scan(n, rate_hz, t0=rng.uniform(0, 3600.0), phi0=rng.uniform(0, 2 * math.pi))
+        dets.append(dict(vec_orig=rotate_beam(beam.vec_orig, pol, r_off, p_off),
+                         beam_vals=beam.beam_vals, theta=th, phi=ph, psi=ps, center=(0.0, 0.0),
+                         fwhm_arcmin=fwhm, ellipticity=ell, pol_angle=pol, offset=(r_off, p_off)))
+    sky = white_sky(nside, seed, dtype=np.float32)
+    return dets, sky

@@ -209,6 +209,17 @@ int todgpu_ring_table_build(int64_t nside, double reach, void *table, size_t byt
 int todgpu_pack_map(const void *planar, int32_t planar_dtype, int64_t C, int64_t N, int64_t stride,
                     int32_t packed_dtype, void *out, void *stream);
 
+/* Spherical-harmonic synthesis of one real RING map component (healpy
+ * alm2map stand-in for seeded synthetic skies; the reference's benchmark
+ * skies come from healpy.synfast, which is not available here): alm is a
+ * device array of (lmax+1)(lmax+2)/2 complex float64 (re, im) pairs in m-major
+ * order (index m (2 lmax + 1 - m)/2 + l); map[comp * map_stride + p] receives
+ * the value at pixel p.  workspace: todgpu_alm2map_workspace_bytes(nside, lmax)
+ * bytes of device memory, overwritten. */
+size_t todgpu_alm2map_workspace_bytes(int64_t nside, int32_t lmax);
+int todgpu_alm2map(int64_t nside, int32_t lmax, const void *alm, void *workspace, size_t ws_bytes,
+                   double *map, int64_t map_stride, int32_t comp, void *stream);
+
 /* FP64 pipe throughput probe (measurement helper; no counterpart in the
  * reference): launches `blocks` CTAs of 256 threads running `iters` rounds of
  * 8 independent FMA chains; *flops receives the floating-point operation count

@@ -105,6 +105,10 @@ def _declare(lib):
     lib.todgpu_ring_table_build.restype = ctypes.c_int
     lib.todgpu_pack_map.argtypes = [_p, _i32, _i64, _i64, _i64, _i32, _p, _p]
     lib.todgpu_pack_map.restype = ctypes.c_int
+    lib.todgpu_alm2map_workspace_bytes.argtypes = [_i64, _i32]
+    lib.todgpu_alm2map_workspace_bytes.restype = ctypes.c_size_t
+    lib.todgpu_alm2map.argtypes = [_i64, _i32, _p, _p, ctypes.c_size_t, _p, _i64, _i32, _p]
+    lib.todgpu_alm2map.restype = ctypes.c_int
     lib.todgpu_fp64_probe.argtypes = [_i64, _i32, _p, ctypes.POINTER(ctypes.c_double), _p]
     lib.todgpu_fp64_probe.restype = ctypes.c_int
     lib.todgpu_abi_version.argtypes = []
@@ -155,6 +159,8 @@ def exported_symbols():
         "todgpu_ring_table_bytes",
         "todgpu_ring_table_build",
         "todgpu_pack_map",
+        "todgpu_alm2map_workspace_bytes",
+        "todgpu_alm2map",
         "todgpu_fp64_probe",
         "todgpu_abi_version",
         "todgpu_last_error_string",

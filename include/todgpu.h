@@ -227,6 +227,74 @@ int todgpu_alm2map(int64_t nside, int32_t lmax, const void *alm, void *workspace
  * never written in practice.  Time it with CUDA events on `stream`. */
 int todgpu_fp64_probe(int64_t blocks, int32_t iters, double *sink, double *flops, void *stream);
 
+/*
+ * Learned far-sidelobe tail (no counterpart in the reference, whose only
+ * tail reduction is the k-means clustering of beam_cluster.py:215-397; the
+ * main lobe keeps going through todgpu_gather_accum).  A Fourier-feature MLP
+ * maps the pointing to the tail's I/Q/U TOD contribution:
+ *   x = (sin t cos p, sin t sin p, cos t, cos psi, sin psi, cos 2psi, sin 2psi)
+ *   f = [cos(2 pi freq x), sin(2 pi freq x)]        freq: (n_freq, 7) float32
+ *   a_1 = silu(W_0 f + b_0), a_{l+1} = silu(W_l a_l + b_l), y = W_D a_D + b_D
+ * with W_0 (width, 2 n_freq), W_l (width, width) for l = 1..depth-1, W_D
+ * (n_out, width).  `params` is the flat float32 parameter vector, per layer
+ * W then b (todgpu_mlp_param_offsets); `params_bf16` its bfloat16 copy, which
+ * the contractions read (float32 accumulation) -- refresh it with
+ * todgpu_mlp_sync_bf16 after writing `params`; the Adam step keeps both.
+ * Constraints: n_freq a multiple of 64, width a multiple of 128, depth in
+ * [1, 8], n_out in [1, 4]; batch row counts (`rows`, `batch`, `chunk`) are
+ * multiples of 128.  Workspaces are device memory of
+ * todgpu_mlp_workspace_bytes(net, rows) bytes, overwritten.
+ */
+typedef struct todgpu_mlp {
+  int32_t n_freq, width, depth, n_out;
+  const float *freq;         /* (n_freq, 7), device */
+  float *params;             /* flat float32, device */
+  void *params_bf16;         /* flat bfloat16, device */
+  float *grad;               /* flat float32 (training only) */
+  float *adam_m, *adam_v;    /* flat float32 Adam moments (training only) */
+} todgpu_mlp;
+
+int64_t todgpu_mlp_param_count(const todgpu_mlp *net);
+/* w_off[l], b_off[l] for l = 0..depth (depth = the head). */
+int todgpu_mlp_param_offsets(const todgpu_mlp *net, int64_t *w_off, int64_t *b_off);
+size_t todgpu_mlp_workspace_bytes(const todgpu_mlp *net, int64_t rows);
+/* Byte offsets of the workspace regions: inputs (rows, 7) f32, features
+ * (rows, 2 n_freq) bf16, pre-activations (depth, rows, width) f32,
+ * activations (depth, rows, width) bf16, head output / its gradient (rows,
+ * n_out) f32, two (rows, width) bf16 gradient buffers, split partial sums,
+ * per-row loss; offsets[8] = total bytes. */
+int todgpu_mlp_workspace_offsets(const todgpu_mlp *net, int64_t rows, int64_t *offsets);
+int todgpu_mlp_sync_bf16(const todgpu_mlp *net, void *stream);
+/* x (rows, 7) float32 from n pointings theta, phi, psi (angles_dtype
+ * TODGPU_F32 or TODGPU_F64); rows n..rows-1 are zeroed. */
+int todgpu_mlp_inputs(const void *theta, const void *phi, const void *psi, int32_t angles_dtype, int64_t n,
+                      int64_t rows, float *x, void *stream);
+/* y (rows, n_out) float32 = network(x). */
+int todgpu_mlp_forward(const todgpu_mlp *net, const float *x, int64_t rows, void *ws, size_t ws_bytes, float *y,
+                       void *stream);
+/* Mean squared error over the batch against target (rows, n_out) into *loss
+ * (device float, optional) and its gradient into net->grad (overwritten). */
+int todgpu_mlp_loss_grad(const todgpu_mlp *net, const float *x, const float *target, int64_t rows, void *ws,
+                         size_t ws_bytes, float *loss, void *stream);
+/* One Adam step (step counts from 1) from net->grad. */
+int todgpu_mlp_adam(const todgpu_mlp *net, int64_t step, float lr, float beta1, float beta2, float eps,
+                    void *stream);
+/* Steps first_step .. first_step+n_steps-1 of Adam (0.9, 0.999, 1e-8) on
+ * consecutive batches of `batch` rows of (x, target) (n_rows a multiple of
+ * batch, batches taken cyclically), learning rate lr_min + (lr_max - lr_min)
+ * (1 + cos(pi step / total_steps)) / 2; loss_per_step (device, n_steps
+ * floats, optional) receives each step's loss. */
+int todgpu_mlp_train(const todgpu_mlp *net, const float *x, const float *target, int64_t n_rows, int64_t batch,
+                     int64_t first_step, int64_t n_steps, int64_t total_steps, float lr_max, float lr_min, void *ws,
+                     size_t ws_bytes, float *loss_per_step, void *stream);
+/* tod[rows[o] * tod_stride + b] += y_o(theta_b, phi_b, psi_b) scale[o] + shift[o]
+ * for b < B, evaluated in chunks of `chunk` samples (rows, scale, shift: host
+ * arrays of n_out entries). */
+int todgpu_tail_accumulate(const todgpu_mlp *net, const void *theta, const void *phi, const void *psi,
+                           int32_t angles_dtype, int64_t B, const int32_t *rows, const double *scale,
+                           const double *shift, double *tod, int64_t tod_stride, int64_t chunk, void *ws,
+                           size_t ws_bytes, void *stream);
+
 /* Library introspection. */
 int todgpu_abi_version(void);
 const char *todgpu_last_error_string(void);

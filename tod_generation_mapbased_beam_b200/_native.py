@@ -68,6 +68,27 @@ class GatherArgs(ctypes.Structure):
     ]
 
 
+class MlpDesc(ctypes.Structure):
+    """Mirror of ``todgpu_mlp`` (include/todgpu.h)."""
+
+    _fields_ = [
+        ("n_freq", _i32),
+        ("width", _i32),
+        ("depth", _i32),
+        ("n_out", _i32),
+        ("freq", _p),
+        ("params", _p),
+        ("params_bf16", _p),
+        ("grad", _p),
+        ("adam_m", _p),
+        ("adam_v", _p),
+    ]
+
+
+# workspace regions of todgpu_mlp_workspace_offsets, in order
+MLP_WS_REGIONS = ("x", "feat", "z", "a", "y", "dz", "part", "loss")
+
+
 class TodGpuError(RuntimeError):
     """A libtodgpu call returned an error status."""
 
@@ -111,6 +132,31 @@ def _declare(lib):
     lib.todgpu_alm2map.restype = ctypes.c_int
     lib.todgpu_fp64_probe.argtypes = [_i64, _i32, _p, ctypes.POINTER(ctypes.c_double), _p]
     lib.todgpu_fp64_probe.restype = ctypes.c_int
+    mp = ctypes.POINTER(MlpDesc)
+    lib.todgpu_mlp_param_count.argtypes = [mp]
+    lib.todgpu_mlp_param_count.restype = _i64
+    lib.todgpu_mlp_param_offsets.argtypes = [mp, _p, _p]
+    lib.todgpu_mlp_param_offsets.restype = ctypes.c_int
+    lib.todgpu_mlp_workspace_bytes.argtypes = [mp, _i64]
+    lib.todgpu_mlp_workspace_bytes.restype = ctypes.c_size_t
+    lib.todgpu_mlp_workspace_offsets.argtypes = [mp, _i64, _p]
+    lib.todgpu_mlp_workspace_offsets.restype = ctypes.c_int
+    lib.todgpu_mlp_sync_bf16.argtypes = [mp, _p]
+    lib.todgpu_mlp_sync_bf16.restype = ctypes.c_int
+    lib.todgpu_mlp_inputs.argtypes = [_p, _p, _p, _i32, _i64, _i64, _p, _p]
+    lib.todgpu_mlp_inputs.restype = ctypes.c_int
+    lib.todgpu_mlp_forward.argtypes = [mp, _p, _i64, _p, ctypes.c_size_t, _p, _p]
+    lib.todgpu_mlp_forward.restype = ctypes.c_int
+    lib.todgpu_mlp_loss_grad.argtypes = [mp, _p, _p, _i64, _p, ctypes.c_size_t, _p, _p]
+    lib.todgpu_mlp_loss_grad.restype = ctypes.c_int
+    lib.todgpu_mlp_adam.argtypes = [mp, _i64, ctypes.c_float, ctypes.c_float, ctypes.c_float, ctypes.c_float, _p]
+    lib.todgpu_mlp_adam.restype = ctypes.c_int
+    lib.todgpu_mlp_train.argtypes = [mp, _p, _p, _i64, _i64, _i64, _i64, _i64, ctypes.c_float, ctypes.c_float,
+                                     _p, ctypes.c_size_t, _p, _p]
+    lib.todgpu_mlp_train.restype = ctypes.c_int
+    lib.todgpu_tail_accumulate.argtypes = [mp, _p, _p, _p, _i32, _i64, _p, _p, _p, _p, _i64, _i64, _p,
+                                           ctypes.c_size_t, _p]
+    lib.todgpu_tail_accumulate.restype = ctypes.c_int
     lib.todgpu_abi_version.argtypes = []
     lib.todgpu_abi_version.restype = ctypes.c_int
     lib.todgpu_last_error_string.argtypes = []
@@ -162,6 +208,17 @@ def exported_symbols():
         "todgpu_alm2map_workspace_bytes",
         "todgpu_alm2map",
         "todgpu_fp64_probe",
+        "todgpu_mlp_param_count",
+        "todgpu_mlp_param_offsets",
+        "todgpu_mlp_workspace_bytes",
+        "todgpu_mlp_workspace_offsets",
+        "todgpu_mlp_sync_bf16",
+        "todgpu_mlp_inputs",
+        "todgpu_mlp_forward",
+        "todgpu_mlp_loss_grad",
+        "todgpu_mlp_adam",
+        "todgpu_mlp_train",
+        "todgpu_tail_accumulate",
         "todgpu_abi_version",
         "todgpu_last_error_string",
     ]

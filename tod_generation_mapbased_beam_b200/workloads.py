@@ -170,3 +170,43 @@ def config4(n_det=64, seed=4, n_min=1e5, n_max=9e6, nside=2048, beam_nside=2048,
                          fwhm_arcmin=fwhm, ellipticity=ell, pol_angle=pol, offset=(r_off, p_off)))
     sky = white_sky(nside, seed, dtype=np.float32)
     return dets, sky
+
+
+def _weights_sum_to(w, total):
+    w = np.asarray(w, np.float64)
+    return (w * (total / w.sum())).astype(np.float32)
+
+
+def config5_beams(beam_nside=2048, seed=5, fwhm_arcmin=30.0, main_fwhm=1.5, tail_deg=(10.0, 20.0), alpha=3.0,
+                  m_max=8, tail_power=0.01):
+    """Learned-tail form (config 5): a Gaussian main lobe (FWHM ``fwhm_arcmin``)
+    kept within ``main_fwhm`` FWHMs of the pole, and a far-sidelobe annulus
+    ``tail_deg`` carrying ``tail_power`` of the beam with a power-law radial
+    falloff r^-alpha times a seeded azimuthal modulation
+    1 + sum_{m <= m_max} a_m cos(m phi + phi_m), a_m ~ U(0, 0.1).  Pixel centres
+    at ``beam_nside``.  Returns (main, tail) :class:`Beam` objects whose weights
+    sum to 1 - tail_power and tail_power."""
+    rng = np.random.default_rng(seed)
+    f = fwhm_arcmin * ARCMIN
+    r_main = main_fwhm * f
+    r_in, r_out = (math.radians(d) for d in tail_deg)
+    n_rings = int(beam_nside * math.sqrt(3.0 * (1.0 - math.cos(r_out)))) + 2
+    if n_rings >= beam_nside:
+        raise ValueError("tail radius reaches past the polar cap; use a smaller tail radius")
+    theta, phi = north_cap_pixel_centres(beam_nside, n_rings)
+    st, ct = np.sin(theta), np.cos(theta)
+    vec = np.stack([st * np.cos(phi), st * np.sin(phi), ct], -1)
+    ra = np.zeros((3, 3))
+    dec = np.full((3, 3), math.pi / 2)
+    m_sel = theta <= r_main
+    sigma = f / math.sqrt(8 * math.log(2))
+    main = Beam(vec[m_sel].astype(np.float32),
+                _weights_sum_to(np.exp(-0.5 * (theta[m_sel] / sigma) ** 2), 1.0 - tail_power), ra, dec,
+                float(theta[m_sel].max()))
+    t_sel = (theta >= r_in) & (theta <= r_out)
+    am = rng.uniform(0.0, 0.1, m_max)
+    phm = rng.uniform(0.0, 2 * math.pi, m_max)
+    mod = 1.0 + sum(am[m - 1] * np.cos(m * phi[t_sel] + phm[m - 1]) for m in range(1, m_max + 1))
+    tail = Beam(vec[t_sel].astype(np.float32), _weights_sum_to(theta[t_sel] ** -alpha * mod, tail_power), ra, dec,
+                float(theta[t_sel].max()))
+    return main, tail

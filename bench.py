@@ -65,6 +65,8 @@ def parse_args():
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-mixed", action="store_true", help="skip the mixed-precision forms")
     p.add_argument("--no-learned", action="store_true", help="skip the learned-tail form (config 5)")
+    p.add_argument("--no-precision", action="store_true", help="skip the nside 2048 precision form (config 3)")
+    p.add_argument("--no-batched", action="store_true", help="skip the 64-detector batched form (config 4)")
     p.add_argument("--learned-train", type=int, default=1 << 18,
                    help="training pointings of the learned tail (plain-method targets)")
     p.add_argument("--no-tables", action="store_true",
@@ -500,7 +502,114 @@ def run_ours(args, dist):
     return result, B, S
 
 
-def run_learned(args, dist):
+def _evt_ms(fn, stream):
+    import torch
+
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    fn()
+    e1.record(stream)
+    e1.synchronize()
+    return e0.elapsed_time(e1)
+
+
+def _err_uk(a, b):
+    d = (a - b) * 1e6
+    return {"rms_uK": np.sqrt((d ** 2).mean(axis=1)).tolist(), "max_uK": np.abs(d).max(axis=1).tolist()}
+
+
+def run_precision(args, dist, sky):
+    """Precision form (config 3): nside 2048 synfast-like sky (seed 2) as
+    packed float32 and bfloat16 records, 30' beam at nside 4096 with a 0.999
+    cut, 8.64e6 scan samples with the rotation derived on the device in
+    float64; one timed launch per form (each ~4 s) after one warm-up, errors
+    on 4096 samples against the float64 path on the same inputs."""
+    import torch
+
+    from tod_generation_mapbased_beam_b200 import _native
+    from tod_generation_mapbased_beam_b200 import workloads as W
+    from tod_generation_mapbased_beam_b200.kernels import gather_accum_angles, pack_map
+
+    dev = torch.device("cuda", dist.local)
+    stream = torch.cuda.current_stream(dev)
+    beam = W.pole_gaussian_beam(30.0, 4096, 0.999, search_fwhm=2.0)
+    B = args.samples
+    th, ph, ps = W.spin_scan(B, 100.0, phi0=0.7 * dist.rank)
+    ang = [torch.from_numpy(a).to(dev) for a in (th, ph, ps)]
+    vec = torch.from_numpy(beam.vec_orig.astype(np.float64)).to(dev)
+    bv = torch.from_numpy(beam.beam_vals).to(dev)
+    interp = _native.BILINEAR if args.mode == "bilinear" else _native.NEAREST
+    idx = torch.from_numpy(np.linspace(0, B - 1, 4096).astype(np.int64)).to(dev)
+    out, subs = {}, {}
+    for kind in ("f64", "f32", "bf16"):
+        mp = sky if kind == "f64" else pack_map(sky, kind)
+        tod = torch.zeros((3, B), dtype=torch.float64, device=dev)
+
+        def launch():
+            tod.zero_()
+            gather_accum_angles(interp, vec, *ang, 0.0, 0.0, 2048, mp, bv, tod, c_q=1, c_u=2)
+
+        launch()
+        ms = dist.max(_evt_ms(launch, stream))
+        subs[kind] = tod[:, idx].cpu().numpy()
+        out[kind] = {"value": B * dist.world / (ms / 1e3), "ms_per_step": ms,
+                     "map": {"f64": "planar float64", "f32": "packed f32 records (16 B/pixel)",
+                             "bf16": "packed bf16 records (8 B/pixel)"}[kind]}
+        del tod, mp
+    for kind in ("f32", "bf16"):
+        out[kind].update(_err_uk(subs[kind], subs["f64"]))
+    return {"workload": f"config3 precision form, {args.mode}: nside 2048 synfast-like sky (seed 2), 30' "
+                        f"beam @ nside 4096, 0.999 cut (S={beam.S}), 100 Hz scan, angles (FP64 rotation "
+                        "on the device)", "samples_per_gpu": B, "S": beam.S, "forms": out,
+            "error_reference": "float64 map, same kernel and pointing (the FP64 path, within 1e-10 of "
+                               "the FP64 CPU oracle in the tests); 4096 samples spread over the day"}
+
+
+def run_batched(args, dist, sky):
+    """Batched form (config 4): 64 detectors (FWHM 25-35', ellipticity 0-0.1,
+    polarisation angle, boresight offset within 1 deg, scans log-uniform in
+    1e5-9e6 samples) on the nside 2048 sky as packed float32 records, one
+    persistent graph-captured launch with the autotuned tile, against one
+    launch per detector."""
+    import torch
+
+    from tod_generation_mapbased_beam_b200 import autotune
+    from tod_generation_mapbased_beam_b200 import workloads as W
+    from tod_generation_mapbased_beam_b200.batched import DetectorBatch
+    from tod_generation_mapbased_beam_b200.kernels import gather_accum_angles, pack_map
+
+    dev = torch.device("cuda", dist.local)
+    stream = torch.cuda.current_stream(dev)
+    dets, _ = W.config4(seed=4, make_sky=False)
+    pm = pack_map(sky, "f32")
+    batch = DetectorBatch(2048, pm, dets, interp_mode=args.mode)
+    t0 = time.perf_counter()
+    batch.tile = autotune.choose_tile(batch, timing_batch=batch.truncated(1.0 / 16))
+    tune_s = time.perf_counter() - t0
+    batch.run()  # graph capture
+    torch.cuda.synchronize()
+    times = [_evt_ms(batch.run, stream) for _ in range(args.steps)]
+    ms = dist.max(statistics.mean(times))
+    n, evals = batch.n_samples, batch.n_evals
+
+    def loop():
+        for d, vec, bvt, angs, o in zip(dets, batch.vec, batch.beam, batch.angles, batch.out):
+            o.zero_()
+            gather_accum_angles(batch.interp, vec, *angs, 0.0, 0.0, 2048, pm, bvt, o, c_q=1, c_u=2)
+
+    loop_ms = dist.max(_evt_ms(loop, stream))
+    batch.release()
+    return {"workload": f"config4 batched, {args.mode}: {len(dets)} detectors, own beams (S "
+                        f"{min(v.shape[0] for v in batch.vec)}-{max(v.shape[0] for v in batch.vec)}), "
+                        "scans log-uniform 1e5-9e6 samples, nside 2048 packed f32 sky",
+            "value": n * dist.world / (ms / 1e3), "unit": "samples/s", "samples_per_gpu": n,
+            "evals_per_s": evals * dist.world / (ms / 1e3), "ms_per_step": ms, "tile": batch.tile,
+            "autotune_seconds": tune_s, "graph": True,
+            "per_detector_launches_value": n * dist.world / (loop_ms / 1e3)}
+
+
+def run_learned(args, dist, sky):
     """Learned-tail form (config 5): nside 2048 synfast-like sky (seed 2),
     30' Gaussian main lobe kept exact within 45' (packed float32 map, Kahan
     sums, float64 decisions) plus a 10-20 deg far-sidelobe annulus with 1% of
@@ -512,14 +621,9 @@ def run_learned(args, dist):
     import torch
 
     from tod_generation_mapbased_beam_b200 import learned as L
-    from tod_generation_mapbased_beam_b200 import sky as SKY
     from tod_generation_mapbased_beam_b200 import workloads as W
 
     dev = torch.device("cuda", dist.local)
-    t0 = time.perf_counter()
-    sky = SKY.synfast_iqu(2048, seed=2)
-    torch.cuda.synchronize()
-    sky_s = time.perf_counter() - t0
     main, tail = W.config5_beams()
     lt = L.LearnedTailTOD(2048, sky, main, tail)
     info = lt.fit(n_train=args.learned_train)
@@ -580,7 +684,7 @@ def run_learned(args, dist):
                     "achieved": round(net_tflops, 2), "unit": "TFLOP/s", "peak": bf16_peak,
                     "frac": round(net_tflops / bf16_peak, 4),
                     "peak_source": f"bf16 dense GEMM burst ({peak_src}); hidden layers on mma.sync bf16"},
-        "training": dict(info, sky_seconds=sky_s, sigma=list(lt.net.sigma)),
+        "training": dict(info, sigma=list(lt.net.sigma)),
     }
 
 
@@ -629,17 +733,29 @@ def main():
 
     dist = Dist()
     res, B, S = run_ours(args, dist)
-    if not args.no_learned:
+    if not (args.no_learned and args.no_precision and args.no_batched):
         import torch
 
+        from tod_generation_mapbased_beam_b200 import sky as SKY
+
         torch.cuda.empty_cache()
-        res["learned"] = run_learned(args, dist)
+        t0 = time.perf_counter()
+        sky2048 = SKY.synfast_iqu(2048, seed=2)  # configs 3-5
+        torch.cuda.synchronize()
+        res["sky2048_seconds"] = time.perf_counter() - t0
+        if not args.no_precision:
+            res["precision"] = run_precision(args, dist, sky2048)
+        if not args.no_batched:
+            res["batched"] = run_batched(args, dist, sky2048)
+        if not args.no_learned:
+            res["learned"] = run_learned(args, dist, sky2048)
+        del sky2048
     if dist.rank == 0:
         line = dict(base, value=res["value"], n_gpus=dist.world, ms_per_step=res["ms_per_step"],
                     scaling="weak", config=dict(config, S=S, parallelism=f"samples x{dist.world}"),
                     roofline=res["roofline"], gpu_launches=res["gpu_launches"],
                     clocks=res["clocks"])
-        for key in ("e2e", "e2e_drop_in", "mixed", "learned"):
+        for key in ("e2e", "e2e_drop_in", "mixed", "precision", "batched", "learned", "sky2048_seconds"):
             if key in res:
                 line[key] = res[key]
         if "cpu_baseline" in res:

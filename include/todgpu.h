@@ -126,8 +126,10 @@ int todgpu_gather_accum(const todgpu_gather_args *args, void *stream);
  * independent gathers -- typically one detector each, with its own beam
  * (vec_orig, beam_vals, S), pointing (B samples) and output tod -- that share
  * interp, nside, the component layout (C, c_q, c_u), params_dtype, map_dtype
- * and flags.  Each job's samples are cut into tiles of `tile` samples; the
- * tiles of all jobs are spread over the persistent grid in contiguous ranges.
+ * and flags.  Each job's samples are cut into tiles of `tile` samples (1 to
+ * 2^24); the tiles of all jobs, numbered job by job, are dealt to the CTAs of
+ * the persistent grid in turn (CTA k takes tiles k, k + G, ...), so that CTAs
+ * running together work on neighbouring samples of one job.
  * Results equal one todgpu_gather_accum call per job.  Up to 96 jobs travel
  * in one launch's parameters; more are split over consecutive launches.
  * Replaces a loop of beam_tod_batch calls over detectors (the reference has

@@ -39,7 +39,7 @@ def test_batched_equals_per_detector(small_config4, mode):
     dets, sky = small_config4
     interp = _native.BILINEAR if mode == "bilinear" else _native.NEAREST
     ref = _single(dets, sky, 128, interp)
-    for tile in (32, 8192):
+    for tile in (1, 32, 8192):
         batch = DetectorBatch(128, sky, dets, interp_mode=mode, tile=tile, graph=False)
         got = [o.cpu().numpy() for o in batch.run()]
         for g, r in zip(got, ref):
@@ -95,3 +95,19 @@ def test_autotuner_picks_and_caches(small_config4, tmp_path, monkeypatch):
     assert autotune.choose_tile(batch) == tile  # served from the cache
     out = batch.run()  # run() autotunes when no tile is given (cache hit here)
     assert batch.tile == tile and len(out) == len(dets)
+
+
+def test_truncated_batch_is_a_prefix_and_tunes_for_the_full_key(small_config4, tmp_path, monkeypatch):
+    dets, sky = small_config4
+    monkeypatch.setenv("TODGPU_AUTOTUNE_CACHE", str(tmp_path / "tune.json"))
+    full = DetectorBatch(128, sky, dets, graph=False, tile=128)
+    ref = [o.clone() for o in full.run()]
+    part = full.truncated(0.25)
+    assert part.n_samples < full.n_samples
+    part.launch(128)
+    for o_part, o_full in zip(part.out, ref):
+        m = o_part.shape[1]
+        assert torch.equal(o_part, o_full[:, :m])  # same samples, same values
+    tile = autotune.choose_tile(full, timing_batch=full.truncated(0.25))
+    data = json.loads((tmp_path / "tune.json").read_text())
+    assert list(data) == [autotune._key(full)] and data[autotune._key(full)]["tile"] == tile

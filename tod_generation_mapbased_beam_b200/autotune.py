@@ -1,8 +1,9 @@
 """Autotuner of the batched launch's tile size.
 
-The tile (samples per work tile) sets how finely the persistent grid splits
-the batch: small tiles balance the CTAs best, large ones keep more of a
-detector's consecutive samples on one CTA.  ``choose_tile`` times each
+The tile (samples per work tile) sets how many consecutive samples of a
+detector a CTA takes at a time: tile 1 spreads neighbouring samples over all
+CTAs (they share the sky region in L2), larger tiles keep runs of samples on
+one CTA (they share it in L1).  ``choose_tile`` times each
 candidate on the actual batch with CUDA events (two launches each, best
 kept) and caches the winner in a JSON file keyed by GPU, nside, map type,
 interpolation mode, detector count and sample/beam-pixel scale, so later runs
@@ -18,7 +19,7 @@ import os
 
 import torch
 
-CANDIDATES = (32, 128, 512, 2048, 8192)
+CANDIDATES = (1, 4, 16, 64, 256)
 
 
 def cache_path():
@@ -55,12 +56,16 @@ def _store(cache):
         pass  # a read-only home only disables the cache
 
 
-def choose_tile(batch, candidates=CANDIDATES, use_cache=True):
-    """Tile size with the shortest launch for ``batch`` (cached)."""
+def choose_tile(batch, candidates=CANDIDATES, use_cache=True, timing_batch=None):
+    """Tile size with the shortest launch for ``batch`` (cached under the
+    batch's key).  ``timing_batch`` (e.g. ``batch.truncated(1 / 16)``) is
+    timed instead of the batch itself when given."""
     key = _key(batch)
     cache = _load() if use_cache else {}
     if key in cache:
         return int(cache[key]["tile"])
+    if timing_batch is not None:
+        batch = timing_batch
     stream = torch.cuda.current_stream()
     timings = {}
     for t in candidates:

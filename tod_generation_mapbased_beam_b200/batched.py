@@ -93,6 +93,20 @@ class DetectorBatch:
             a.ring_table = None if self.table is None else self.table.data_ptr()
         return arr
 
+    def truncated(self, fraction):
+        """A batch over the first ``fraction`` of every detector's samples that
+        shares this batch's device buffers (a cheaper stand-in with the same
+        detectors and the same proportions, e.g. for timing tile sizes)."""
+        import copy
+
+        b = copy.copy(self)
+        b.angles = [[t[:max(1, int(t.shape[0] * fraction))] for t in ang] for ang in self.angles]
+        b.out = [o[:, :a[0].shape[0]] for o, a in zip(self.out, b.angles)]
+        b._args = b._make_args()
+        b._graph = None
+        b.tile = None
+        return b
+
     def launch(self, tile=None):
         """Zero the outputs and launch once on the current stream (no graph)."""
         for o in self.out:

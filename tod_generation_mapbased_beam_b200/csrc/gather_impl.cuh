@@ -875,13 +875,14 @@ __device__ __forceinline__ void flush_sample(const KArgs& a, const double* s_red
   }
 }
 
-// Samples b = b_begin, b_begin + b_step, ... < b_end of one job (one beam
-// entry over one batch of samples), by the whole CTA.  With a ring table:
+// Samples of tiles t = t_begin, t_begin + t_step, ... < t_end of one job (one
+// beam entry over one batch of samples; tile t holds samples [t tile,
+// min(B, (t + 1) tile))), by the whole CTA.  With a ring table:
 // ring data come from it and, when the entry carries Q and U, each sample's
 // footprint gets a spin-2 table in shared memory.  Without one: everything is
 // evaluated directly.  All threads of the CTA must call it together.
 template <int MODE, bool HAS_QU, typename MapT, int PM, int LAYOUT, int NT>
-__device__ void run_samples(const KArgs& a, long long b_begin, long long b_end, long long b_step,
+__device__ void run_samples(const KArgs& a, long long t_begin, long long t_end, long long t_step, long long tile,
                             unsigned char* smem_raw, double* s_red) {
   constexpr int NW = NT / 32;
   Spin2Tab& w = *reinterpret_cast<Spin2Tab*>(smem_raw);
@@ -915,7 +916,8 @@ __device__ void run_samples(const KArgs& a, long long b_begin, long long b_end, 
   }
   unsigned long long nerr = 0;
   long long prev = -1;
-  for (long long b = b_begin; b < b_end; b += b_step) {
+  for (long long t = t_begin; t < t_end; t += t_step)
+  for (long long b = t * tile, b_stop = min(a.B, (t + 1) * tile); b < b_stop; ++b) {
     const SampleRot rot = load_rot<PM>(a, b);
     Bore bo{0.0, 0.0, 0.0};
     if (HAS_QU) load_boresight<PM>(a, rot, b, bo.z, bo.sth, bo.phi);
@@ -1025,14 +1027,19 @@ template <int MODE, bool HAS_QU, typename MapT, int PM, int LAYOUT, int NT, int 
 __global__ void __launch_bounds__(NT, MINB) gather_accum_kernel(const KArgs a) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   __shared__ double s_red[(NT / 32) * 4];
-  run_samples<MODE, HAS_QU, MapT, PM, LAYOUT, NT>(a, blockIdx.x, a.B, gridDim.x, smem_raw, s_red);
+  run_samples<MODE, HAS_QU, MapT, PM, LAYOUT, NT>(a, blockIdx.x, a.B, gridDim.x, 1, smem_raw, s_red);
 }
 
 // Many jobs (detectors: each its own beam, pointing, output and length) in
 // one persistent launch.  Job j's samples form tiles of `tile` samples; the
-// T tiles of all jobs are numbered job by job and CTA k takes the contiguous
-// tile range [k T / G, (k + 1) T / G), so consecutive samples of one job stay
-// on one CTA.  The descriptors travel in the kernel parameters.
+// tiles of all jobs are numbered job by job (tiles_before[j] = tiles of jobs
+// 0..j-1) and CTA k takes tiles k, k + G, k + 2G, ... (G = grid size), as one
+// launch per job with its samples interleaved over the CTAs would, without a
+// launch boundary between jobs.  CTAs running at the same time then work on
+// neighbouring samples of one job (the same sky region, shared in L2), and
+// every CTA gets an equal share of every job whatever its beam size.  `tile`
+// sets how many consecutive samples a CTA takes at a time.  The descriptors
+// travel in the kernel parameters.
 constexpr int kMaxBatchJobs = 96;
 struct BatchParams {
   int njobs;
@@ -1045,20 +1052,13 @@ template <int MODE, bool HAS_QU, typename MapT, int PM, int LAYOUT, int NT, int 
 __global__ void __launch_bounds__(NT, MINB) gather_batched_kernel(const __grid_constant__ BatchParams p) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   __shared__ double s_red[(NT / 32) * 4];
-  const long long T = p.tiles_before[p.njobs];
-  const long long t_lo = (long long)blockIdx.x * T / gridDim.x;
-  const long long t_hi = ((long long)blockIdx.x + 1) * T / gridDim.x;
-  long long t = t_lo;
-  int j = 0;
-  while (t < t_hi) {
-    while (j < p.njobs - 1 && p.tiles_before[j + 1] <= t) ++j;
-    const KArgs& a = p.job[j];
-    // all tiles of job j in this CTA's range, as one run
-    const long long t_end = min(t_hi, p.tiles_before[j + 1]);
-    const long long b0 = (t - p.tiles_before[j]) * p.tile;
-    const long long b1 = min(a.B, (t_end - p.tiles_before[j]) * p.tile);
-    run_samples<MODE, HAS_QU, MapT, PM, LAYOUT, NT>(a, b0, b1, 1, smem_raw, s_red);
-    t = t_end;
+  const long long G = gridDim.x, k = blockIdx.x;
+  for (int j = 0; j < p.njobs; ++j) {
+    const long long ntiles = p.tiles_before[j + 1] - p.tiles_before[j];
+    // first tile of job j that falls to this CTA: global index = k (mod G)
+    const long long t0 = ((k - p.tiles_before[j]) % G + G) % G;
+    if (t0 < ntiles)
+      run_samples<MODE, HAS_QU, MapT, PM, LAYOUT, NT>(p.job[j], t0, ntiles, G, p.tile, smem_raw, s_red);
   }
 }
 

@@ -491,7 +491,7 @@ extern "C" int todgpu_gather_accum_batched(const todgpu_gather_args* jobs, int32
   if (njobs < 0) return fail(TODGPU_ESHAPE, "njobs < 0");
   if (njobs == 0) return TODGPU_OK;
   if (!jobs) return fail(TODGPU_EINVAL, "jobs is NULL");
-  if (tile < 1) return fail(TODGPU_ESHAPE, "tile must be >= 1 sample");
+  if (tile < 1 || tile > (1LL << 24)) return fail(TODGPU_ESHAPE, "tile must be in [1, 2^24] samples");
   const todgpu_gather_args& j0 = jobs[0];
   for (int j = 0; j < njobs; ++j) {
     const todgpu_gather_args& a = jobs[j];

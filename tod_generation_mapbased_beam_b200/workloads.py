@@ -146,13 +146,14 @@ def rotate_beam(vec, pol_angle, offset_theta, offset_phi):
     return v * ca + np.cross(k, v) * sa + np.outer(v @ k, k) * (1 - ca)
 
 
-def config4(n_det=64, seed=4, n_min=1e5, n_max=9e6, nside=2048, beam_nside=2048, rate_hz=100.0):
+def config4(n_det=64, seed=4, n_min=1e5, n_max=9e6, nside=2048, beam_nside=2048, rate_hz=100.0, make_sky=True):
     """Batched form (config 4): detectors with their own beam (FWHM ~ U(25', 35'),
     ellipticity ~ U(0, 0.1), polarisation angle ~ U(0, pi)), boresight offset
     uniform in a 1 deg disc and a scan length ~ log-uniform in [n_min, n_max];
     a float32 sky.  Returns (detectors, sky); each detector is a dict with
     ``vec_orig`` (float64, offset beam), ``beam_vals``, ``theta, phi, psi``
-    (float32 scan of its own length and phase) and ``center`` (0, 0)."""
+    (float32 scan of its own length and phase) and ``center`` (0, 0).  With
+    ``make_sky=False`` the sky is None (the caller brings its own)."""
     rng = np.random.default_rng(seed)
     dets = []
     for d in range(n_det):
@@ -168,7 +169,7 @@ def config4(n_det=64, seed=4, n_min=1e5, n_max=9e6, nside=2048, beam_nside=2048,
         dets.append(dict(vec_orig=rotate_beam(beam.vec_orig, pol, r_off, p_off),
                          beam_vals=beam.beam_vals, theta=th, phi=ph, psi=ps, center=(0.0, 0.0),
                          fwhm_arcmin=fwhm, ellipticity=ell, pol_angle=pol, offset=(r_off, p_off)))
-    sky = white_sky(nside, seed, dtype=np.float32)
+    sky = white_sky(nside, seed, dtype=np.float32) if make_sky else None
     return dets, sky
 
 

@@ -297,6 +297,34 @@ int todgpu_tail_accumulate(const todgpu_mlp *net, const void *theta, const void 
                            const double *shift, double *tod, int64_t tod_stride, int64_t chunk, void *ws,
                            size_t ws_bytes, void *stream);
 
+/*
+ * Weighted spherical k-means of beam pixels (the clustering of
+ * beam_cluster.py:70-188, used by cluster_beam_pixels :215-397).  vec (S, 3)
+ * float64 unit vectors and w (S,) float64 weights are device arrays; S < 2^31,
+ * 1 <= K <= 8192 clusters.  Workspaces: todgpu_kmeans_workspace_bytes(S, K)
+ * bytes of device memory, overwritten.
+ *
+ * todgpu_kmeans_seed: k-means++ seeding (beam_cluster.py:70-112).  Centroid k
+ * is pixel i, the first index with cumsum(p)_i / sum(p) > uniforms[k] (a host
+ * array of K draws in [0, 1), the caller's random stream), p_i = w_i for
+ * k = 0 and w_i max(1 - max_{j<k} v_i . c_j, 0)^2 after that (w when all
+ * p_i are 0).  centroids (K, 3) and chosen (K,) int64 are device outputs.
+ * todgpu_kmeans_assign: labels[i] = argmax_k v_i . c_k (first maximum),
+ * best[i] = the maximum, with v . c = fma(v2, c2, fma(v1, c1, v0 c0)).
+ * todgpu_kmeans_sums: sums (K, 4) = per cluster (sum w x, sum w y, sum w z,
+ * sum w), each taken in increasing pixel order (as numpy.bincount does).
+ * todgpu_kmeans_argmin: first index of the minimum of best (S,) into *index
+ * (device int64).
+ */
+size_t todgpu_kmeans_workspace_bytes(int64_t S, int32_t K);
+int todgpu_kmeans_seed(const double *vec, const double *w, int64_t S, int32_t K, const double *uniforms,
+                       double *centroids, int64_t *chosen, void *ws, size_t ws_bytes, void *stream);
+int todgpu_kmeans_assign(const double *vec, int64_t S, const double *centroids, int32_t K, int32_t *labels,
+                         double *best, void *stream);
+int todgpu_kmeans_sums(const double *vec, const double *w, const int32_t *labels, int64_t S, int32_t K,
+                       double *sums, void *ws, size_t ws_bytes, void *stream);
+int todgpu_kmeans_argmin(const double *best, int64_t S, int64_t *index, void *stream);
+
 /* Library introspection. */
 int todgpu_abi_version(void);
 const char *todgpu_last_error_string(void);

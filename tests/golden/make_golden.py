@@ -298,7 +298,48 @@ def beam_prep_case():
     return out
 
 
+def clusters_case():
+    """cluster_beam_pixels (beam_cluster.py:215-397) on larger inputs: full
+    mode and hybrid mode on a pixelised Gaussian beam, full mode on a
+    power-law annulus with an azimuthal modulation (a far-sidelobe tail)."""
+    out = {}
+    nside = 512
+    # pixel centres of RING rings 1..n (north cap) as unit vectors
+    th, ph = [], []
+    for i in range(1, 60):
+        z = 1.0 - i * i / (3.0 * nside * nside)
+        j = np.arange(4 * i)
+        th.append(np.full(4 * i, math.acos(z)))
+        ph.append((j + 0.5) * (math.pi / (2 * i)))
+    th = np.concatenate(th)
+    ph = np.concatenate(ph)
+    vec = np.stack([np.sin(th) * np.cos(ph), np.sin(th) * np.sin(ph), np.cos(th)], -1)
+    g = np.exp(-0.5 * (th / 0.02) ** 2) * (1 + 0.3 * np.cos(2 * ph))
+    sel = g > 1e-3 * g.max()
+    gv = vec[sel].astype(np.float32)
+    gb = (g[sel] / g[sel].sum()).astype(np.float32)
+    ring = (th > 0.05) & (th < 0.1)
+    tv = vec[ring].astype(np.float32)
+    tb = (th[ring] ** -3.0 * (1 + 0.08 * np.cos(3 * ph[ring] + 0.4)))
+    tb = (tb / tb.sum()).astype(np.float32)
+    cases = {"gauss_full_64": (gv, gb, 64, None), "gauss_hybrid_40": (gv, gb, 40, 0.3),
+             "annulus_full_200": (tv, tb, 200, None), "gauss_full_3": (gv, gb, 3, None)}
+    for name, (v, b, k, tf) in cases.items():
+        vo, bo, lab = bc.cluster_beam_pixels(v, b, n_clusters=k, tail_fraction=tf, verbose=False)
+        out[f"{name}__vec_in"] = v
+        out[f"{name}__bv_in"] = b
+        out[f"{name}__k"] = np.int64(k)
+        out[f"{name}__tail_fraction"] = np.float64(-1.0 if tf is None else tf)
+        out[f"{name}__vec"] = vo
+        out[f"{name}__bv"] = bo
+        out[f"{name}__labels"] = lab
+    return out
+
+
 def main():
+    if "--only-clusters" in sys.argv:
+        np.savez_compressed(os.path.join(HERE, "clusters.npz"), **clusters_case())
+        return
     np.savez_compressed(os.path.join(HERE, "kernels.npz"),
                         **{f"{c}__{k}": v for c, d in kernel_cases().items() for k, v in d.items()})
     np.savez_compressed(os.path.join(HERE, "healpix.npz"),
@@ -307,6 +348,7 @@ def main():
     np.savez_compressed(os.path.join(HERE, "rotations.npz"), **rotation_case())
     np.savez_compressed(os.path.join(HERE, "core.npz"), **core_case())
     np.savez_compressed(os.path.join(HERE, "beam_prep.npz"), **beam_prep_case())
+    np.savez_compressed(os.path.join(HERE, "clusters.npz"), **clusters_case())
     for f in sorted(os.listdir(HERE)):
         if f.endswith(".npz"):
             print(f, os.path.getsize(os.path.join(HERE, f)))

@@ -157,6 +157,16 @@ def _declare(lib):
     lib.todgpu_tail_accumulate.argtypes = [mp, _p, _p, _p, _i32, _i64, _p, _p, _p, _p, _i64, _i64, _p,
                                            ctypes.c_size_t, _p]
     lib.todgpu_tail_accumulate.restype = ctypes.c_int
+    lib.todgpu_kmeans_workspace_bytes.argtypes = [_i64, _i32]
+    lib.todgpu_kmeans_workspace_bytes.restype = ctypes.c_size_t
+    lib.todgpu_kmeans_seed.argtypes = [_p, _p, _i64, _i32, _p, _p, _p, _p, ctypes.c_size_t, _p]
+    lib.todgpu_kmeans_seed.restype = ctypes.c_int
+    lib.todgpu_kmeans_assign.argtypes = [_p, _i64, _p, _i32, _p, _p, _p]
+    lib.todgpu_kmeans_assign.restype = ctypes.c_int
+    lib.todgpu_kmeans_sums.argtypes = [_p, _p, _p, _i64, _i32, _p, _p, ctypes.c_size_t, _p]
+    lib.todgpu_kmeans_sums.restype = ctypes.c_int
+    lib.todgpu_kmeans_argmin.argtypes = [_p, _i64, _p, _p]
+    lib.todgpu_kmeans_argmin.restype = ctypes.c_int
     lib.todgpu_abi_version.argtypes = []
     lib.todgpu_abi_version.restype = ctypes.c_int
     lib.todgpu_last_error_string.argtypes = []
@@ -219,6 +229,11 @@ def exported_symbols():
         "todgpu_mlp_adam",
         "todgpu_mlp_train",
         "todgpu_tail_accumulate",
+        "todgpu_kmeans_workspace_bytes",
+        "todgpu_kmeans_seed",
+        "todgpu_kmeans_assign",
+        "todgpu_kmeans_sums",
+        "todgpu_kmeans_argmin",
         "todgpu_abi_version",
         "todgpu_last_error_string",
     ]

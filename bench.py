@@ -69,6 +69,7 @@ def parse_args():
     p.add_argument("--no-batched", action="store_true", help="skip the 64-detector batched form (config 4)")
     p.add_argument("--learned-train", type=int, default=1 << 18,
                    help="training pointings of the learned tail (plain-method targets)")
+    p.add_argument("--learned-steps", type=int, default=4000, help="training steps of the learned tail")
     p.add_argument("--no-tables", action="store_true",
                    help="evaluate ring data and spin-2 angles directly (A/B comparison)")
     p.add_argument("--cpu-seconds", type=float, default=10.0,
@@ -369,9 +370,11 @@ def run_ours(args, dist):
 
     def step():
         tod.zero_()
+        torch.cuda.nvtx.range_push("plain_step")
         k0.record(stream)
         _native.check(lib.todgpu_gather_accum(ctypes.byref(cargs), stream.cuda_stream))
         k1.record(stream)
+        torch.cuda.nvtx.range_pop()
 
     k0 = torch.cuda.Event(enable_timing=True)
     k1 = torch.cuda.Event(enable_timing=True)
@@ -626,7 +629,7 @@ def run_learned(args, dist, sky):
     dev = torch.device("cuda", dist.local)
     main, tail = W.config5_beams()
     lt = L.LearnedTailTOD(2048, sky, main, tail)
-    info = lt.fit(n_train=args.learned_train)
+    info = lt.fit(n_train=args.learned_train, steps=args.learned_steps)
     B = args.samples
     th, ph, ps = W.spin_scan(B, 100.0, phi0=0.7 * dist.rank)
     idx = np.linspace(0, B - 1, 4096).astype(np.int64)
@@ -639,11 +642,13 @@ def run_learned(args, dist, sky):
     main_ms, net_ms = [], []
     for i in range(args.warmup + args.steps):
         tod.zero_()
+        torch.cuda.nvtx.range_push("learned_form")
         ev[0].record(stream)
         lt.main_lobe(*scan, tod)
         ev[1].record(stream)
         lt.learned_tail(*scan, tod)
         ev[2].record(stream)
+        torch.cuda.nvtx.range_pop()
         ev[2].synchronize()
         if i >= args.warmup:
             main_ms.append(ev[0].elapsed_time(ev[1]))

@@ -1086,15 +1086,24 @@ constexpr size_t kTabHeaderBytes = (sizeof(Spin2Tab) + 15) & ~size_t(15);
 #ifndef TODGPU_CTA_THREADS
 #define TODGPU_CTA_THREADS 256
 #endif
-#ifndef TODGPU_CTA_MINB
-#define TODGPU_CTA_MINB 4  // 64 registers; 3 (80 registers) measured 0.3-5% slower
-#endif
 constexpr int kNT = TODGPU_CTA_THREADS;  // threads per CTA
-constexpr int kMinB = TODGPU_CTA_MINB;   // CTAs per SM the register budget is sized for
+
+// CTAs per SM the register budget is sized for: 4 (64 registers) for the
+// nearest mode and packed maps, where the fourth CTA measured 3-5% faster; 3
+// (80 registers) for bilinear on planar maps, where it gained nothing and the
+// extra spilling doubled the local-memory write-back to DRAM.
+template <int MODE, typename MapT>
+constexpr int min_blocks() {
+#ifdef TODGPU_CTA_MINB
+  return TODGPU_CTA_MINB;
+#else
+  return (MODE == TODGPU_NEAREST || MapTraits<MapT>::packed) ? 4 : 3;
+#endif
+}
 
 template <int MODE, bool HAS_QU, typename MapT, int PM, int LAYOUT>
 int launch_gather(KArgs k, cudaStream_t stream) {
-  auto kern = gather_accum_kernel<MODE, HAS_QU, MapT, PM, LAYOUT, kNT, kMinB>;
+  auto kern = gather_accum_kernel<MODE, HAS_QU, MapT, PM, LAYOUT, kNT, min_blocks<MODE, MapT>()>;
   static LaunchInfo info;
   static std::mutex mu;
   using TabT = typename MapTraits<MapT>::Tab;
@@ -1129,7 +1138,7 @@ static_assert(sizeof(BatchParams) <= 32000, "batched descriptors must fit the ke
 // Batched launch: descriptors of up to kMaxBatchJobs jobs per launch.
 template <int MODE, bool HAS_QU, typename MapT, int PM, int LAYOUT>
 int launch_batched(BatchParams& bp, bool any_table, cudaStream_t stream) {
-  auto kern = gather_batched_kernel<MODE, HAS_QU, MapT, PM, LAYOUT, kNT, kMinB>;
+  auto kern = gather_batched_kernel<MODE, HAS_QU, MapT, PM, LAYOUT, kNT, min_blocks<MODE, MapT>()>;
   static LaunchInfo info;
   static std::mutex mu;
   using TabT = typename MapTraits<MapT>::Tab;

@@ -256,6 +256,21 @@ typedef struct todgpu_mlp {
   float *adam_m, *adam_v;    /* flat float32 Adam moments (training only) */
 } todgpu_mlp;
 
+/* Forward product of the hidden layers: TODGPU_MLP_TCGEN05 (default: 5th-
+ * generation tensor cores, float32 accumulators in tensor memory; widths 128
+ * and 256) or TODGPU_MLP_MMA_SYNC (warp-level tensor-core instructions; any
+ * width, and the path the backward products always take).  Process-wide;
+ * returns the previous setting.  todgpu_mlp_wait_timeouts: number of bounded
+ * waits in the tcgen05 kernel that ran out since load (0 in a healthy run;
+ * reading it synchronises the device), -1 on a CUDA error. */
+#define TODGPU_MLP_TCGEN05 0
+#define TODGPU_MLP_MMA_SYNC 1
+int todgpu_mlp_set_forward_path(int32_t path);
+int64_t todgpu_mlp_wait_timeouts(void);
+/* Number of forward layers launched on the tcgen05 path since load (a layer
+ * whose shape or tensor maps do not suit it runs on mma.sync instead). */
+int64_t todgpu_mlp_tcgen05_launches(void);
+
 int64_t todgpu_mlp_param_count(const todgpu_mlp *net);
 /* w_off[l], b_off[l] for l = 0..depth (depth = the head). */
 int todgpu_mlp_param_offsets(const todgpu_mlp *net, int64_t *w_off, int64_t *b_off);

@@ -203,3 +203,37 @@ def test_bad_rows_rejected(TN):
     x = torch.zeros((100, 7), dtype=torch.float32, device="cuda")
     with pytest.raises((_native.TodGpuError, ValueError)):
         net.forward(x)
+
+
+@pytest.mark.parametrize("width", [128, 256])
+def test_tcgen05_forward_matches_mma_sync_forward(TN, width):
+    from tod_generation_mapbased_beam_b200 import _native
+
+    lib = _native.lib()
+    net = TN.TailNet(128, width, 3, 3, sigma=(2.0, 1.0), seed=17)
+    th, ph, ps = _pointings(4096, 18)
+    x = net.inputs(th, ph, ps)
+    prev = lib.todgpu_mlp_set_forward_path(_native.MLP_MMA_SYNC)
+    try:
+        y_ref = net.forward(x).double().cpu().numpy()
+        a_ref = _bf16_region(net, 4096, "a", (3, 4096, width))
+        lib.todgpu_mlp_set_forward_path(_native.MLP_TCGEN05)
+        n0 = lib.todgpu_mlp_tcgen05_launches()
+        y_tc = net.forward(x).double().cpu().numpy()
+        assert lib.todgpu_mlp_tcgen05_launches() == n0 + 3  # every hidden layer ran on tcgen05
+        a_tc = _bf16_region(net, 4096, "a", (3, 4096, width))
+    finally:
+        lib.todgpu_mlp_set_forward_path(prev)
+    assert lib.todgpu_mlp_wait_timeouts() == 0
+    # same bf16 operands, float32 sums in a different order: activations agree
+    # to a bf16 rounding step, the outputs to float32 sums
+    diff = a_tc != a_ref
+    assert diff.mean() < 0.02
+    assert np.all(np.abs(a_tc - a_ref) <= 2.0 ** -6 * np.abs(a_ref) + 1e-6)
+    assert np.abs(y_tc - y_ref).max() <= 1e-3 * np.abs(y_ref).max()
+
+
+def test_forward_path_switch_rejects_unknown():
+    from tod_generation_mapbased_beam_b200 import _native
+
+    assert _native.lib().todgpu_mlp_set_forward_path(7) == _native.EINVAL

@@ -85,6 +85,8 @@ class MlpDesc(ctypes.Structure):
     ]
 
 
+MLP_TCGEN05, MLP_MMA_SYNC = 0, 1  # forward paths of todgpu_mlp_set_forward_path
+
 # workspace regions of todgpu_mlp_workspace_offsets, in order
 MLP_WS_REGIONS = ("x", "feat", "z", "a", "y", "dz", "part", "loss")
 
@@ -157,6 +159,12 @@ def _declare(lib):
     lib.todgpu_tail_accumulate.argtypes = [mp, _p, _p, _p, _i32, _i64, _p, _p, _p, _p, _i64, _i64, _p,
                                            ctypes.c_size_t, _p]
     lib.todgpu_tail_accumulate.restype = ctypes.c_int
+    lib.todgpu_mlp_set_forward_path.argtypes = [_i32]
+    lib.todgpu_mlp_set_forward_path.restype = ctypes.c_int
+    lib.todgpu_mlp_wait_timeouts.argtypes = []
+    lib.todgpu_mlp_wait_timeouts.restype = _i64
+    lib.todgpu_mlp_tcgen05_launches.argtypes = []
+    lib.todgpu_mlp_tcgen05_launches.restype = _i64
     lib.todgpu_kmeans_workspace_bytes.argtypes = [_i64, _i32]
     lib.todgpu_kmeans_workspace_bytes.restype = ctypes.c_size_t
     lib.todgpu_kmeans_seed.argtypes = [_p, _p, _i64, _i32, _p, _p, _p, _p, ctypes.c_size_t, _p]
@@ -218,6 +226,9 @@ def exported_symbols():
         "todgpu_alm2map_workspace_bytes",
         "todgpu_alm2map",
         "todgpu_fp64_probe",
+        "todgpu_mlp_set_forward_path",
+        "todgpu_mlp_wait_timeouts",
+        "todgpu_mlp_tcgen05_launches",
         "todgpu_mlp_param_count",
         "todgpu_mlp_param_offsets",
         "todgpu_mlp_workspace_bytes",

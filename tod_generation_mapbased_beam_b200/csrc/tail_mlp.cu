@@ -11,16 +11,21 @@
 //   y     = W_D a_D + b_D                             W_D: (O, H)
 // Weights are used in bfloat16 (a copy of the float32 master parameters that
 // the Adam step refreshes), activations are stored in bfloat16 and every
-// contraction accumulates in float32: the hidden layers on the tensor cores
-// (mma.sync m16n8k16 bf16 -> f32, operands staged in shared memory), the
-// O <= 4 wide head on the CUDA cores.  Pre-activations are kept in float32 for
+// contraction accumulates in float32: the hidden layers on the tensor cores --
+// forward products on tcgen05 with TMEM accumulators and TMA-staged operands
+// (widths 128 and 256), backward products and other widths on mma.sync
+// m16n8k16 bf16 -> f32 -- the O <= 4 wide head on the CUDA cores.  Pre-activations are kept in float32 for
 // the backward pass.  Weight gradients over the batch use a fixed split of
 // the batch and a fixed-order reduction, so training is deterministic.
+#include <cuda.h>
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
+#include <cudaTypedefs.h>
 
 #include <algorithm>
+#include <atomic>
 #include <cmath>
+#include <mutex>
 
 #include "gather_impl.cuh"
 
@@ -460,6 +465,219 @@ __global__ void to_bf16_kernel(const float* p, bf16* pb, long long n) {
 }
 
 // ---------------------------------------------------------------------------
+// Forward layer on the 5th-generation tensor cores (tcgen05, sm_100a), with
+// its operands staged by the tensor memory accelerator (TMA):
+//   out(m, n) = silu(sum_k A(m, k) W(n, k) + bias(n)),  A (M, K), W (N, K)
+//   bf16 row-major; the sums accumulate in float32 in tensor memory (TMEM).
+// One CTA of 256 threads per 128-row tile, all N (128 or 256) columns at once
+// in N TMEM columns.  K advances in k-tiles of 32 through a ring of 4 shared-
+// memory stages.  Lane 0 of warp 0 is the producer and the MMA issuer: it
+// starts the TMA copies of a k-tile (A: 128 x 32, W: N x 32) on the stage's
+// "full" barrier (transaction count = the stage's bytes), waits for them,
+// issues the k-tile's two 128 x N x 16 MMAs and commits them to the stage's
+// "empty" barrier, and refills the stage of the previous k-tile once that
+// barrier shows its MMAs done.  The tensor maps view each operand as
+// (8 elements, rows, K / 8) with strides (2 B, K * 2 B, 16 B), so a box of
+// (8, rows, 4) lands in shared memory in the canonical no-swizzle K-major
+// layout: 8-row x 16-byte core matrices, 8-row groups 128 B apart, 16-byte K
+// chunks one column of row groups apart.  Epilogue: warp w reads TMEM lanes
+// 32 (w % 4) .. +31 (its rows) and half of the columns, adds the bias, applies
+// SiLU, stores bfloat16 (and the float32 pre-activation when asked).  Every
+// wait is bounded; a wait that runs out is counted in g_tc_timeouts and the
+// CTA skips the rest of its work, still freeing its TMEM.
+// ---------------------------------------------------------------------------
+constexpr int TC_BM = 128, TC_BK = 32, TC_STAGES = 4, TC_THREADS = 256;
+constexpr int kTcWaitLimit = 1 << 20;
+__device__ unsigned int g_tc_timeouts;
+
+template <int N>
+struct TcShape {
+  static constexpr int A_BYTES = TC_BM * TC_BK * 2;      // 8 KB
+  static constexpr int B_BYTES = N * TC_BK * 2;          // 8 or 16 KB
+  static constexpr int STAGE = A_BYTES + B_BYTES;
+  static constexpr int SMEM = TC_STAGES * STAGE;
+  static constexpr int A_LBO = (TC_BM / 8) * 128;        // byte stride between K chunks
+  static constexpr int B_LBO = (N / 8) * 128;
+  // instruction descriptor, kind::f16: D f32 (bits 4-5 = 1), A and B bf16
+  // (bits 7-9, 10-12 = 1), both K-major, N >> 3 at bit 17, M >> 4 at bit 24
+  static constexpr uint32_t IDESC = (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(N >> 3) << 17) |
+                                    ((uint32_t)(TC_BM >> 4) << 24);
+};
+
+// shared-memory matrix descriptor: start >> 4 (bits 0-13), leading byte offset
+// >> 4 (bits 16-29), stride byte offset >> 4 (bits 32-45), version 1 (bit 46),
+// no swizzle (bits 61-63 = 0)
+__device__ __forceinline__ uint64_t tc_desc(uint32_t addr, uint32_t lbo, uint32_t sbo) {
+  return (uint64_t)((addr >> 4) & 0x3FFFu) | ((uint64_t)((lbo >> 4) & 0x3FFFu) << 16) |
+         ((uint64_t)((sbo >> 4) & 0x3FFFu) << 32) | (1ull << 46);
+}
+
+__device__ __forceinline__ bool tc_wait(uint32_t bar, uint32_t parity) {
+  for (int it = 0; it < kTcWaitLimit; ++it) {
+    uint32_t done;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\tselp.b32 %0, 1, 0, p;\n\t}"
+        : "=r"(done)
+        : "r"(bar), "r"(parity)
+        : "memory");
+    if (done) return true;
+  }
+  return false;
+}
+
+// TMA copies of k-tile kt (A rows m0.., all N rows of W) into stage st.
+template <int N>
+__device__ __forceinline__ void tc_produce(const CUtensorMap* ta, const CUtensorMap* tw, long long m0, int kt,
+                                           uint32_t stage_addr, uint32_t full_bar) {
+  using Sh = TcShape<N>;
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%1], %0;" ::"r"((uint32_t)Sh::STAGE), "r"(full_bar)
+               : "memory");
+  const int kc = kt * (TC_BK / 8);
+  asm volatile(
+      "cp.async.bulk.tensor.3d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%3, %4, %5}], [%2];" ::
+          "r"(stage_addr),
+      "l"(reinterpret_cast<uint64_t>(ta)), "r"(full_bar), "r"(0), "r"((int)m0), "r"(kc)
+      : "memory");
+  asm volatile(
+      "cp.async.bulk.tensor.3d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%3, %4, %5}], [%2];" ::
+          "r"(stage_addr + (uint32_t)Sh::A_BYTES),
+      "l"(reinterpret_cast<uint64_t>(tw)), "r"(full_bar), "r"(0), "r"(0), "r"(kc)
+      : "memory");
+}
+
+template <int N>
+__global__ void __launch_bounds__(TC_THREADS) gemm_tc_fwd_kernel(const __grid_constant__ CUtensorMap tma_a,
+                                                                 const __grid_constant__ CUtensorMap tma_w, int K,
+                                                                 const float* bias, float* zout, bf16* aout,
+                                                                 long long ldc) {
+  using Sh = TcShape<N>;
+  extern __shared__ __align__(1024) unsigned char tc_smem[];
+  __shared__ __align__(8) unsigned long long bars[2 * TC_STAGES + 1];  // full[S], empty[S], done
+  __shared__ uint32_t tmem_slot;
+  __shared__ int s_ok;
+  __shared__ float s_bias[N];
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const long long m0 = (long long)blockIdx.x * TC_BM;
+  const uint32_t sbase = (uint32_t)__cvta_generic_to_shared(tc_smem);
+  const uint32_t bar0 = (uint32_t)__cvta_generic_to_shared(bars);
+  const uint32_t full0 = bar0, empty0 = bar0 + 8 * TC_STAGES, done = bar0 + 16 * TC_STAGES;
+  for (int i = tid; i < N; i += TC_THREADS) s_bias[i] = bias[i];
+  if (tid == 0) {
+    for (int i = 0; i < 2 * TC_STAGES + 1; ++i)
+      asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(bar0 + 8 * i));
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    s_ok = 1;
+  }
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
+                     (uint32_t)__cvta_generic_to_shared(&tmem_slot)),
+                 "r"(N));
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+  const uint32_t tmem = tmem_slot;
+
+  if (warp == 0) {
+    if (lane == 0) {
+      const int KT = K / TC_BK;
+      bool ok = true;
+      int produced = 0, consumed = 0;  // k-tiles whose copies were started / waited for
+      for (int kt = 0; kt < TC_STAGES && kt < KT; ++kt, ++produced)
+        tc_produce<N>(&tma_a, &tma_w, m0, kt, sbase + kt * Sh::STAGE, full0 + 8 * kt);
+      for (int kt = 0; kt < KT && ok; ++kt) {
+        const int st = kt % TC_STAGES;
+        const uint32_t sa = sbase + st * Sh::STAGE, sb = sa + Sh::A_BYTES;
+        if (!tc_wait(full0 + 8 * st, (uint32_t)((kt / TC_STAGES) & 1))) {
+          ok = false;
+          break;
+        }
+        consumed = kt + 1;
+        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+#pragma unroll
+        for (int s = 0; s < TC_BK / 16; ++s) {
+          const uint64_t da = tc_desc(sa + s * 2 * Sh::A_LBO, Sh::A_LBO, 128);
+          const uint64_t db = tc_desc(sb + s * 2 * Sh::B_LBO, Sh::B_LBO, 128);
+          const uint32_t accumulate = (kt > 0 || s > 0) ? 1u : 0u;
+          asm volatile(
+              "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+              "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}" ::"r"(tmem),
+              "l"(da), "l"(db), "r"(Sh::IDESC), "r"(accumulate));
+        }
+        asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+                         empty0 + 8 * st)
+                     : "memory");
+        // refill the previous k-tile's stage once its MMAs are done
+        const int kp = kt - 1, kr = kp + TC_STAGES;
+        if (kp >= 0 && kr < KT) {
+          const int sp = kp % TC_STAGES;
+          if (!tc_wait(empty0 + 8 * sp, (uint32_t)((kp / TC_STAGES) & 1))) {
+            ok = false;
+            break;
+          }
+          tc_produce<N>(&tma_a, &tma_w, m0, kr, sbase + sp * Sh::STAGE, full0 + 8 * sp);
+          ++produced;
+        }
+      }
+      // after a timeout: let copies already started land before the CTA leaves
+      for (int t = consumed; !ok && t < produced; ++t)
+        tc_wait(full0 + 8 * (t % TC_STAGES), (uint32_t)((t / TC_STAGES) & 1));
+      if (ok) {
+        asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(done)
+                     : "memory");
+        ok = tc_wait(done, 0);
+      }
+      if (!ok) {
+        s_ok = 0;
+        atomicAdd(&g_tc_timeouts, 1u);
+      }
+    }
+    __syncwarp();
+  }
+  __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+  if (s_ok) {
+    const int q = warp & 3, half = warp >> 2;
+    const long long row = m0 + q * 32 + lane;
+#pragma unroll 1
+    for (int c0 = half * (N / 2); c0 < (half + 1) * (N / 2); c0 += 32) {
+      uint32_t r[32];
+      asm volatile(
+          "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, "
+          "%14, %15, %16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, %28, %29, %30, %31}, [%32];"
+          : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+            "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15]),
+            "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]),
+            "=r"(r[23]), "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]),
+            "=r"(r[30]), "=r"(r[31])
+          : "r"(tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)c0));
+      asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+      float v[32];
+#pragma unroll
+      for (int j = 0; j < 32; ++j) v[j] = __uint_as_float(r[j]) + s_bias[c0 + j];
+      if (zout) {
+        float4* zp = reinterpret_cast<float4*>(zout + row * ldc + c0);
+#pragma unroll
+        for (int j = 0; j < 8; ++j) zp[j] = make_float4(v[4 * j], v[4 * j + 1], v[4 * j + 2], v[4 * j + 3]);
+      }
+      uint4* ap = reinterpret_cast<uint4*>(aout + row * ldc + c0);
+#pragma unroll
+      for (int j = 0; j < 4; ++j) {
+        __nv_bfloat162 h[4];
+#pragma unroll
+        for (int t = 0; t < 4; ++t)
+          h[t] = __floats2bfloat162_rn(silu_f(v[8 * j + 2 * t]), silu_f(v[8 * j + 2 * t + 1]));
+        ap[j] = *reinterpret_cast<const uint4*>(h);
+      }
+    }
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(N));
+}
+
+// ---------------------------------------------------------------------------
 // host orchestration
 // ---------------------------------------------------------------------------
 inline unsigned grid1d(long long n, int threads) {
@@ -505,6 +723,72 @@ inline Ws ws_view(const Dims& d, long long M, void* base) {
 }
 
 // features of w.x, then the hidden layers (pre-activations kept when keep_z).
+// Forward path of the hidden layers: tcgen05 (default) for widths 128 and 256,
+// mma.sync otherwise or when selected by todgpu_mlp_set_forward_path.
+inline std::atomic<int>& forward_path() {
+  static std::atomic<int> path{TODGPU_MLP_TCGEN05};
+  return path;
+}
+
+inline std::atomic<long long>& tc_launch_count() {
+  static std::atomic<long long> n{0};
+  return n;
+}
+
+// cuTensorMapEncodeTiled from the driver, through the runtime (no libcuda link).
+inline PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
+  static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+  static std::once_flag once;
+  std::call_once(once, [] {
+    void* p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+  });
+  return fn;
+}
+
+// (8 elements, rows, K / 8) view of a row-major (rows, K) bf16 matrix, box (8, box_rows, TC_BK / 8).
+inline bool encode_operand(CUtensorMap* map, const bf16* base, long long rows, int K, int box_rows) {
+  auto enc = tensor_map_encoder();
+  if (!enc) return false;
+  const cuuint64_t dims[3] = {8, (cuuint64_t)rows, (cuuint64_t)(K / 8)};
+  const cuuint64_t strides[2] = {(cuuint64_t)K * 2, 16};
+  const cuuint32_t box[3] = {8, (cuuint32_t)box_rows, TC_BK / 8};
+  const cuuint32_t estr[3] = {1, 1, 1};
+  return enc(map, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 3, const_cast<bf16*>(base), dims, strides, box, estr,
+             CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+             CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
+template <int N>
+bool launch_tc(const GemmArgs& g, cudaStream_t s) {
+  static std::once_flag once;
+  static cudaError_t attr = cudaSuccess;
+  std::call_once(once, [] {
+    attr = cudaFuncSetAttribute(gemm_tc_fwd_kernel<N>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                TcShape<N>::SMEM);
+  });
+  if (attr != cudaSuccess) return false;
+  CUtensorMap ta, tw;
+  if (!encode_operand(&ta, g.A, g.M, g.K, TC_BM) || !encode_operand(&tw, g.B, N, g.K, N)) return false;
+  gemm_tc_fwd_kernel<N><<<g.M / TC_BM, TC_THREADS, TcShape<N>::SMEM, s>>>(ta, tw, g.K, g.bias, g.zout, g.aout,
+                                                                        g.ldc);
+  tc_launch_count().fetch_add(1);
+  return true;
+}
+
+// The layer on the tcgen05 path if selected and its shape allows; false: not launched.
+inline bool forward_tc(const GemmArgs& g, cudaStream_t s) {
+  if (forward_path().load() != TODGPU_MLP_TCGEN05 || g.K % TC_BK != 0 || g.M % TC_BM != 0 || g.lda != g.K ||
+      g.ldb != g.K || g.ldc != g.N)
+    return false;
+  if (g.N == 256) return launch_tc<256>(g, s);
+  if (g.N == 128) return launch_tc<128>(g, s);
+  return false;
+}
+
 inline void forward_hidden(const Net& n, const Ws& w, long long M, bool keep_z, cudaStream_t s) {
   const Dims& d = n.d;
   features_kernel<<<grid1d(M * d.F, 256), 256, 0, s>>>(w.x, M, n.freq, d.F, w.feat);
@@ -521,7 +805,7 @@ inline void forward_hidden(const Net& n, const Ws& w, long long M, bool keep_z, 
     g.zout = keep_z ? w.z + (long long)l * M * d.H : nullptr;
     g.aout = w.a + (long long)l * M * d.H;
     g.ldc = d.H;
-    gemm<0, 0, EPI_FWD>(g, 1, s);
+    if (!forward_tc(g, s)) gemm<0, 0, EPI_FWD>(g, 1, s);
   }
 }
 
@@ -849,3 +1133,16 @@ extern "C" int todgpu_tail_accumulate(const todgpu_mlp* m, const void* theta, co
   }
   return finish("tail accumulate");
 }
+
+extern "C" int todgpu_mlp_set_forward_path(int32_t path) {
+  if (path != TODGPU_MLP_TCGEN05 && path != TODGPU_MLP_MMA_SYNC) return fail(TODGPU_EINVAL, "unknown forward path");
+  return forward_path().exchange(path);
+}
+
+extern "C" int64_t todgpu_mlp_wait_timeouts(void) {
+  unsigned int v = 0;
+  if (cudaMemcpyFromSymbol(&v, g_tc_timeouts, sizeof(v)) != cudaSuccess) return -1;
+  return (int64_t)v;
+}
+
+extern "C" int64_t todgpu_mlp_tcgen05_launches(void) { return tc_launch_count().load(); }

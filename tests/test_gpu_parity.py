@@ -257,3 +257,40 @@ def test_beam_tod_angles_api():
     ref = tod_core.beam_tod_batch(nside, None, data, rot, phi, theta, -beta + psi)
     for c in (0, 1, 2):
         assert np.abs(out[c] - ref[c]).max() <= 1e-4 * np.abs(ref[c]).max()
+
+
+@pytest.mark.parametrize("mode", ["bilinear", "nearest"])
+def test_config1_entries_vs_oracle(mode):
+    """Config 1 at full size (1e5 samples, S ~ 250): the I+Q entry (C = 2, no
+    spin-2) and the U entry (C = 1, signed weights) through the drop-in
+    beam_tod_batch with the reference's host pointing preparation, against
+    the C oracle on the same float32 parameters."""
+    from tod_generation_mapbased_beam_b200 import sky as SKY
+    from tod_generation_mapbased_beam_b200 import tod_rotations as R
+    from tod_generation_mapbased_beam_b200 import workloads as W
+
+    cfg = W.config1()
+    nside = cfg["nside"]
+    sky = SKY.synfast_iqu(nside, seed=0).cpu().numpy()
+    ra, dec = cfg["beam"].ra, cfg["beam"].dec
+    rot, beta = R.precompute_rotation_vector_batch(ra, dec, cfg["phi"], cfg["theta"])
+    psis = -beta + cfg["psi"]
+    params = R._rotation_params(rot, cfg["phi"], cfg["theta"], psis)
+    B = len(cfg["phi"])
+    fn = oracle.gather_accum_fused if mode == "bilinear" else oracle.gather_accum_nearest
+    for name, entry in cfg["entries"].items():
+        comps = entry["comp_indices"]
+        data = dict(entry, mp_stacked=np.ascontiguousarray(sky[comps]))
+        res = tod_core.beam_tod_batch(nside, list(sky), data, rot, cfg["phi"], cfg["theta"], psis,
+                                      interp_mode=mode)
+        S = entry["vec_orig"].shape[0]
+        ref = np.zeros((len(comps), B))
+        fn(entry["vec_orig"], *params, nside, data["mp_stacked"], entry["beam_vals"], B, S, ref, -1, -1)
+        scale = np.abs(ref).max()
+        for i, c in enumerate(comps):
+            r32 = ref[i].astype(np.float32)
+            # float64 sums agree to 1e-12 of the largest magnitude, so the
+            # float32 casts agree to 1 ulp (or that absolute bound near zero)
+            bound = np.maximum(np.spacing(np.abs(r32)), 1e-12 * scale)
+            assert np.all(np.abs(res[c].astype(np.float64) - r32) <= bound), (name, c)
+    assert S > 200

@@ -120,6 +120,25 @@ def white_sky(nside, seed, dtype=np.float64):
     return out
 
 
+def config1(n_samples=100_000, rate_hz=20.0):
+    """Plain method, CPU-runnable (config 1): nside 128 sky; an elliptical
+    Gaussian I beam (FWHM 1.8 deg along the beam-frame x axis, 1.5 deg across)
+    at beam nside 256 with a 0.99 power cut; Q beam = I beam, so I and Q share
+    one entry (C = 2, no spin-2); the U beam is 1% of the I beam times
+    sin 2 phi_b on the I selection, normalised by the I beam's sum (signed,
+    zero-mean weights; the reference's normalise-by-sum of such a beam would
+    divide by ~0); a 20 Hz spin scan.  Returns the two beam entries (the
+    reference's data dicts without maps) and the float32 scan."""
+    beam = pole_gaussian_beam(108.0, 256, 0.99, fwhm2_arcmin=90.0, search_fwhm=3.0)
+    v = beam.vec_orig.astype(np.float64)
+    phi_b = np.arctan2(v[:, 1], v[:, 0])
+    u_vals = (0.01 * beam.beam_vals.astype(np.float64) * np.sin(2 * phi_b)).astype(np.float32)
+    iq = dict(vec_orig=beam.vec_orig, beam_vals=beam.beam_vals, comp_indices=[0, 1], ra=beam.ra, dec=beam.dec)
+    u = dict(vec_orig=beam.vec_orig, beam_vals=u_vals, comp_indices=[2], ra=beam.ra, dec=beam.dec)
+    theta, phi, psi = spin_scan(n_samples, rate_hz)
+    return dict(nside=128, entries={"IQ": iq, "U": u}, theta=theta, phi=phi, psi=psi, beam=beam)
+
+
 def config2(n_samples=8_640_000, seed=1):
     """Plain method on GPU (config 2): nside 1024 float64 sky, 30' FWHM
     circular beam at beam nside 2048 with a 0.99 power cut, 100 Hz spin scan."""

@@ -359,11 +359,16 @@ def run_ours(args, dist):
     params = [to(beam.vec_orig)] + [to(p) for p in params_h]
     bore = to(bore_h)
     bv = to(beam.beam_vals)
+    from tod_generation_mapbased_beam_b200.kernels import pack_map
+
     sky = to(wl["sky"])
+    # float64 map as float64 records {I, Q, U, 0}: the library's layout for the
+    # float64 path (packed on upload; TOD bit-identical to the planar map)
+    sky_rec = pack_map(sky, "f64")
     tod = torch.zeros((3, B), dtype=torch.float64, device=dev)
     interp = _native.BILINEAR if args.mode == "bilinear" else _native.NEAREST
     table = None if args.no_tables else ring_table(nside, beam_reach(beam.vec_orig, nside), dev)
-    cargs = make_args(interp, nside, B, S, 3, 1, 2, params, np.float32, bore, bv, sky, tod,
+    cargs = make_args(interp, nside, B, S, 3, 1, 2, params, np.float32, bore, bv, sky_rec, tod,
                       table=table)
     lib = _native.lib()
     stream = torch.cuda.current_stream(dev)
@@ -433,11 +438,10 @@ def run_ours(args, dist):
     # records, float32 spin-2 table, float32 Kahan sum, float64 decisions;
     # error against the FP64 oracle on a bounded subset of samples
     if not args.no_mixed:
-        from tod_generation_mapbased_beam_b200.kernels import pack_map
-
         mixed = {}
-        for kind in ("f32", "bf16"):
-            pm = pack_map(sky, kind)
+        tod_rec = tod.clone()  # the float64 result of the last timed step
+        for kind in ("planar_f64", "f32", "bf16"):
+            pm = sky if kind == "planar_f64" else pack_map(sky, kind)
             margs = make_args(interp, nside, B, S, 3, 1, 2, params, np.float32, bore, bv, pm, tod,
                               table=table)
             for _ in range(2):
@@ -453,8 +457,11 @@ def run_ours(args, dist):
             m1.synchronize()
             mms = dist.max(m0.elapsed_time(m1) / args.steps)
             entry = {"value": B * dist.world / (mms / 1e3), "ms_per_step": mms,
-                     "map": f"packed {kind} records ({16 if kind == 'f32' else 8} B/pixel)"}
-            if dist.rank == 0 and not args.no_cpu_baseline:
+                     "map": {"planar_f64": "planar float64 (C, N), the reference's mp_stacked",
+                             "f32": "packed f32 records (16 B/pixel)", "bf16": "packed bf16 records (8 B/pixel)"}[kind]}
+            if kind == "planar_f64":
+                entry["bit_identical_to_value"] = bool(torch.equal(tod, tod_rec))
+            elif dist.rank == 0 and not args.no_cpu_baseline:
                 entry.update(mixed_error_uk(wl, args.mode, kind, tod, cargs, margs, lib, stream))
             mixed[kind] = entry
         result["mixed"] = mixed
@@ -715,7 +722,7 @@ def main():
             "warmup": args.warmup, "vs_baseline": None, "dtype": "f64",
             "data": "synthetic: seeded 100 Hz spin scan, pole-centred Gaussian beam, seeded "
                     "synfast-like I/Q/U sky (GPU alm2map, C_l^TT ~ (l+10)^-2, 100 uK RMS)"}
-    config = {"workload": f"config2 plain FP64, {args.mode}: nside 1024 f64 I/Q/U sky, 30' FWHM "
+    config = {"workload": f"config2 plain FP64, {args.mode}: nside 1024 f64 I/Q/U sky (float64 records), 30' FWHM "
                           f"beam @ nside 2048 0.99 cut, 100 Hz spin scan, one beam entry (I,Q,U; spin-2)",
               "samples_per_gpu": args.samples, "mode": args.mode,
               "l2": "inputs larger than L2 (params+map ~1 GB), no flush needed",

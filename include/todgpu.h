@@ -51,6 +51,11 @@ extern "C" {
  * float64. */
 #define TODGPU_PACKED_F32 2
 #define TODGPU_PACKED_BF16 3
+/* map_dtype: one record of 4 float64 components per pixel (32 B, 16-byte
+ * aligned), made by todgpu_pack_map: the float64 path with a pixel's I/Q/U
+ * side by side -- same values and arithmetic as a planar float64 map, so the
+ * same results bit for bit, with one memory sector per stencil pixel. */
+#define TODGPU_PACKED_F64 4
 
 /*
  * Arguments of one fused gather/accumulate call: one beam entry over a batch
@@ -204,9 +209,9 @@ size_t todgpu_ring_table_bytes(int64_t nside);
 int todgpu_ring_table_build(int64_t nside, double reach, void *table, size_t bytes, void *stream);
 
 /* Pack a planar (C, N) float32/float64 map (row stride `stride` elements) into
- * N records of 4 components for the precision form: packed_dtype
- * TODGPU_PACKED_F32 (16 B/pixel, `out` 16-byte aligned) or TODGPU_PACKED_BF16
- * (8 B/pixel, round to nearest even).  No counterpart in the reference, which
+ * N records of 4 components: packed_dtype TODGPU_PACKED_F32 (16 B/pixel, `out`
+ * 16-byte aligned), TODGPU_PACKED_BF16 (8 B/pixel, round to nearest even) or
+ * TODGPU_PACKED_F64 (32 B/pixel, exact, `out` 16-byte aligned).  No counterpart in the reference, which
  * reads planar mp_stacked (gridint.py:447-450). */
 int todgpu_pack_map(const void *planar, int32_t planar_dtype, int64_t C, int64_t N, int64_t stride,
                     int32_t packed_dtype, void *out, void *stream);

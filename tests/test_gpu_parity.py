@@ -294,3 +294,45 @@ def test_config1_entries_vs_oracle(mode):
             bound = np.maximum(np.spacing(np.abs(r32)), 1e-12 * scale)
             assert np.all(np.abs(res[c].astype(np.float64) - r32) <= bound), (name, c)
     assert S > 200
+
+
+@pytest.mark.parametrize("mode", ["bilinear", "nearest"])
+def test_packed_f64_map_is_bit_identical(kernel_case, mode):
+    """Float64 records {I, Q, U, 0} give exactly the planar float64 map's TOD
+    (golden kernel cases with float64 maps, with and without the tables)."""
+    from tod_generation_mapbased_beam_b200 import _native
+    from tod_generation_mapbased_beam_b200.kernels import gather_accum, pack_map
+
+    name, g = kernel_case
+    mp = g["mp_stacked"]
+    if mp.dtype != np.float64 or mp.shape[0] > 4:
+        pytest.skip("float64 maps only")
+    interp = _native.BILINEAR if mode == "bilinear" else _native.NEAREST
+    args = [g[k] for k in PARAM_KEYS]
+    for flags in (0, _native.FLAG_NO_TABLES):
+        outs = []
+        for m in (mp, pack_map(mp, "f64")):
+            tod = torch.from_numpy(g["tod_init"].copy()).cuda()
+            gather_accum(interp, *args, int(g["nside"]), m, g["beam_vals"], int(g["B"]), int(g["S"]), tod,
+                         int(g["c_q"]), int(g["c_u"]), flags=flags)
+            outs.append(tod.cpu().numpy())
+        assert np.array_equal(outs[0], outs[1]), (name, flags)
+
+
+@pytest.mark.parametrize("mode", ["bilinear", "nearest"])
+def test_packed_f64_map_bit_identical_device_pointing(mode):
+    from tod_generation_mapbased_beam_b200 import _native
+    from tod_generation_mapbased_beam_b200 import workloads as W
+    from tod_generation_mapbased_beam_b200.kernels import gather_accum_angles, pack_map
+
+    beam = W.pole_gaussian_beam(60.0, 512, 0.99, search_fwhm=1.5)
+    th, ph, ps = W.spin_scan(3000, 100.0, phi0=1.1)
+    sky = W.white_sky(256, 4)
+    interp = _native.BILINEAR if mode == "bilinear" else _native.NEAREST
+    outs = []
+    for m in (sky, pack_map(sky, "f64")):
+        tod = torch.zeros((3, len(th)), dtype=torch.float64, device="cuda")
+        gather_accum_angles(interp, beam.vec_orig.astype(np.float64), th, ph, ps, 0.0, 0.0, 256, m,
+                            beam.beam_vals, tod, 1, 2)
+        outs.append(tod.cpu().numpy())
+    assert np.array_equal(outs[0], outs[1])

@@ -19,7 +19,7 @@ OK = 0
 EINVAL, ENSIDE, ESHAPE, EDTYPE, ECUDA, EABI = -1, -2, -3, -4, -5, -6
 BILINEAR, NEAREST = 0, 1
 F32, F64, ANGLES = 0, 1, 2
-PACKED_F32, PACKED_BF16 = 2, 3
+PACKED_F32, PACKED_BF16, PACKED_F64 = 2, 3, 4
 FLAG_NO_TABLES = 1
 
 _i32 = ctypes.c_int32

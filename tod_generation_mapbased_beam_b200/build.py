@@ -31,7 +31,7 @@ LIB = os.path.join(OUT_DIR, "libtodgpu.so")
 # One translation unit per map element type (they instantiate the gather
 # kernels and compile in parallel) plus the C ABI.
 SOURCES = ["tod_api.cu", "gather_map_f64.cu", "gather_map_f32.cu", "gather_map_pf32.cu",
-           "gather_map_pbf16.cu", "sky_synth.cu", "tail_mlp.cu", "kmeans.cu"]
+           "gather_map_pbf16.cu", "gather_map_pf64.cu", "sky_synth.cu", "tail_mlp.cu", "kmeans.cu"]
 HEADERS = ["healpix_ring.cuh", "gather_impl.cuh"]
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]

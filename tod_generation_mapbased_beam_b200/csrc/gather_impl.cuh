@@ -232,6 +232,7 @@ __device__ __forceinline__ void rotate_pixel(const KArgs& a, const SampleRot& r,
 
 struct PackF32;
 struct PackBF16;
+struct PackF64;
 template <typename MapT>
 __device__ __forceinline__ float4 load_rec(const KArgs& a, long long p);
 __device__ __forceinline__ float rec_at(const float4& r, int c);
@@ -240,6 +241,8 @@ template <typename MapT>
 __device__ __forceinline__ double map_at(const KArgs& a, int c, long long p) {
   if constexpr (std::is_same<MapT, PackF32>::value || std::is_same<MapT, PackBF16>::value)
     return (double)rec_at(load_rec<MapT>(a, p), c);
+  else if constexpr (std::is_same<MapT, PackF64>::value)
+    return __ldg(static_cast<const double*>(a.map) + 4 * p + c);
   else
     return (double)__ldg(static_cast<const MapT*>(a.map) + (long long)c * a.map_stride + p);
 }
@@ -250,6 +253,8 @@ template <typename MapT>
 __device__ __forceinline__ double map_x_beam(const KArgs& a, int c, long long p, float bv) {
   if constexpr (std::is_same<MapT, PackF32>::value || std::is_same<MapT, PackBF16>::value) {
     return (double)(rec_at(load_rec<MapT>(a, p), c) * bv);
+  } else if constexpr (std::is_same<MapT, PackF64>::value) {
+    return __ldg(static_cast<const double*>(a.map) + 4 * p + c) * (double)bv;
   } else {
     const MapT m = __ldg(static_cast<const MapT*>(a.map) + (long long)c * a.map_stride + p);
     if constexpr (sizeof(MapT) == 4)
@@ -265,10 +270,14 @@ __device__ __forceinline__ double map_x_beam(const KArgs& a, int c, long long p,
 // record: PackF32 = 4 x float32 (16 B), PackBF16 = 4 x bfloat16 (8 B).  The
 // precision form also keeps cos 2d / sin 2d in float32 and accumulates in
 // float32 with Kahan compensation; pixel decisions and weights stay float64.
+// PackF64 = 4 x float64 (32 B, one sector) is the float64 path's layout with
+// a pixel's components together: every value and operation as for a planar
+// float64 map, so the results are the same bit for bit.
 // ---------------------------------------------------------------------------
 
 struct PackF32 {};
 struct PackBF16 {};
+struct PackF64 {};
 
 template <typename MapT>
 struct MapTraits {
@@ -697,17 +706,44 @@ struct Chan<kLayoutIQU> {
 
 template <typename MapT>
 __device__ __forceinline__ double map_i(const KArgs& a, int c, int p) {
-  return (double)__ldg(static_cast<const MapT*>(a.map) + (long long)c * a.map_stride + p);
+  if constexpr (std::is_same<MapT, PackF64>::value)
+    return __ldg(static_cast<const double*>(a.map) + 4LL * p + c);
+  else
+    return (double)__ldg(static_cast<const MapT*>(a.map) + (long long)c * a.map_stride + p);
 }
 
 template <typename MapT>
 __device__ __forceinline__ double map_x_beam_i(const KArgs& a, int c, int p, float bv) {
-  const MapT m = __ldg(static_cast<const MapT*>(a.map) + (long long)c * a.map_stride + p);
-  if constexpr (sizeof(MapT) == 4)
-    return (double)(m * bv);
-  else
-    return m * (double)bv;
+  if constexpr (std::is_same<MapT, PackF64>::value) {
+    return __ldg(static_cast<const double*>(a.map) + 4LL * p + c) * (double)bv;
+  } else {
+    const MapT m = __ldg(static_cast<const MapT*>(a.map) + (long long)c * a.map_stride + p);
+    if constexpr (sizeof(MapT) == 4)
+      return (double)(m * bv);
+    else
+      return m * (double)bv;
+  }
 }
+
+// A pixel's map values for the float64 bilinear path: planar maps read each
+// component where it is used; PackF64 records are read as two 16-byte loads.
+template <typename MapT>
+struct PixelVals {
+  const KArgs& a;
+  int p;
+  __device__ __forceinline__ PixelVals(const KArgs& a_, int p_) : a(a_), p(p_) {}
+  __device__ __forceinline__ double operator()(int c) const { return map_i<MapT>(a, c, p); }
+};
+template <>
+struct PixelVals<PackF64> {
+  double2 lo, hi;
+  __device__ __forceinline__ PixelVals(const KArgs& a, int p)
+      : lo(__ldg(static_cast<const double2*>(a.map) + 2LL * p)),
+        hi(__ldg(static_cast<const double2*>(a.map) + 2LL * p + 1)) {}
+  __device__ __forceinline__ double operator()(int c) const {
+    return c == 0 ? lo.x : (c == 1 ? lo.y : (c == 2 ? hi.x : hi.y));
+  }
+};
 
 template <int MODE, bool HAS_QU, typename MapT, int LAYOUT, typename TabT, class Acc>
 __device__ __forceinline__ void eval_fast(const KArgs& a, const Bore& bo, const RingRec* rt, const Spin2Tab& w,
@@ -755,11 +791,12 @@ __device__ __forceinline__ void eval_fast(const KArgs& a, const Bore& bo, const 
     } else {
       double tq = 0.0, tu = 0.0, to[4] = {0.0, 0.0, 0.0, 0.0};
       stencil_fast(nside, z, phi_w, rt, [&](int k, int p, double wk, int ring, int ip, int n, double zn, double phin) {
+        const PixelVals<MapT> pv(a, p);
         if constexpr (HAS_QU) {
           double c2, s2;
           spin2_fast(w, tab, ring, ip, n, zn, phin, bo, c2, s2);
-          const double q = map_i<MapT>(a, ch.q, p);
-          const double u = map_i<MapT>(a, ch.u, p);
+          const double q = pv(ch.q);
+          const double u = pv(ch.u);
           const double vq = wk * fma(q, c2, u * s2);
           const double vu = wk * fma(u, c2, -q * s2);
           tq = (k == 0) ? vq : tq + vq;
@@ -769,7 +806,7 @@ __device__ __forceinline__ void eval_fast(const KArgs& a, const Bore& bo, const 
         for (int c = 0; c < 4; ++c) {
           if (c >= ch.C) break;
           if (HAS_QU && (c == ch.q || c == ch.u)) continue;
-          const double m = map_i<MapT>(a, c, p);
+          const double m = pv(c);
           to[c] = (k == 0) ? wk * m : fma(wk, m, to[c]);
         }
       });
@@ -1208,6 +1245,7 @@ TODGPU_DECLARE_MAP_DISPATCH(f64)
 TODGPU_DECLARE_MAP_DISPATCH(f32)
 TODGPU_DECLARE_MAP_DISPATCH(pf32)
 TODGPU_DECLARE_MAP_DISPATCH(pbf16)
+TODGPU_DECLARE_MAP_DISPATCH(pf64)
 #undef TODGPU_DECLARE_MAP_DISPATCH
 
 #define TODGPU_DEFINE_MAP_DISPATCH(NAME, MAPT)                                                             \

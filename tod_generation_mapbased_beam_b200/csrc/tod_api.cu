@@ -270,6 +270,19 @@ __global__ void __launch_bounds__(kNTStatic) static_reach_kernel(const KArgs a, 
   }
 }
 
+// Planar (C, N) float/double map -> one float64 record of 4 components per
+// pixel (missing components are 0), as two 16-byte stores.
+template <typename SrcT>
+__global__ void pack_map_f64_kernel(const SrcT* src, int C, long long N, long long stride, void* out) {
+  for (long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x; p < N; p += (long long)gridDim.x * blockDim.x) {
+    double v[4] = {0.0, 0.0, 0.0, 0.0};
+    for (int c = 0; c < C; ++c) v[c] = (double)src[(long long)c * stride + p];
+    double2* o = static_cast<double2*>(out) + 2 * p;
+    o[0] = make_double2(v[0], v[1]);
+    o[1] = make_double2(v[2], v[3]);
+  }
+}
+
 // Planar (C, N) float/double map -> one record per pixel of 4 components
 // (float32 or bfloat16, round to nearest even; missing components are 0).
 template <typename SrcT, bool BF16>
@@ -316,6 +329,7 @@ static int dispatch_types(const KArgs& k, int interp, bool has_qu, int map_dtype
   switch (map_dtype) {
     case TODGPU_PACKED_F32: return dispatch_single_pf32(k, interp, has_qu, params_dtype, s);
     case TODGPU_PACKED_BF16: return dispatch_single_pbf16(k, interp, has_qu, params_dtype, s);
+    case TODGPU_PACKED_F64: return dispatch_single_pf64(k, interp, has_qu, params_dtype, s);
     case TODGPU_F32: return dispatch_single_f32(k, interp, has_qu, params_dtype, s);
     default: return dispatch_single_f64(k, interp, has_qu, params_dtype, s);
   }
@@ -326,6 +340,7 @@ static int dispatch_batched(BatchParams& bp, int interp, bool has_qu, bool iqu, 
   switch (map_dtype) {
     case TODGPU_PACKED_F32: return dispatch_batched_pf32(bp, interp, has_qu, iqu, any_table, params_dtype, s);
     case TODGPU_PACKED_BF16: return dispatch_batched_pbf16(bp, interp, has_qu, iqu, any_table, params_dtype, s);
+    case TODGPU_PACKED_F64: return dispatch_batched_pf64(bp, interp, has_qu, iqu, any_table, params_dtype, s);
     case TODGPU_F32: return dispatch_batched_f32(bp, interp, has_qu, iqu, any_table, params_dtype, s);
     default: return dispatch_batched_f64(bp, interp, has_qu, iqu, any_table, params_dtype, s);
   }
@@ -357,13 +372,14 @@ static int check_common(const todgpu_gather_args* a, bool need_map) {
     if (a->c_q < -1 || a->c_q >= a->C || a->c_u < -1 || a->c_u >= a->C)
       return fail(TODGPU_ESHAPE, "c_q/c_u must be -1 or a component index");
     if (a->c_q >= 0 && a->c_q == a->c_u) return fail(TODGPU_ESHAPE, "c_q == c_u");
-    const bool packed = a->map_dtype == TODGPU_PACKED_F32 || a->map_dtype == TODGPU_PACKED_BF16;
+    const bool packed = a->map_dtype == TODGPU_PACKED_F32 || a->map_dtype == TODGPU_PACKED_BF16 ||
+                        a->map_dtype == TODGPU_PACKED_F64;
     if (a->map_dtype != TODGPU_F32 && a->map_dtype != TODGPU_F64 && !packed)
-      return fail(TODGPU_EDTYPE, "map_dtype must be TODGPU_F32, TODGPU_F64, TODGPU_PACKED_F32 or TODGPU_PACKED_BF16");
+      return fail(TODGPU_EDTYPE, "map_dtype must be TODGPU_F32, TODGPU_F64 or a TODGPU_PACKED_* type");
     const long long npix = 12 * a->nside * a->nside;
     if (!packed && a->map_stride < npix) return fail(TODGPU_ESHAPE, "map_stride < 12*nside^2");
-    if (packed && ((uintptr_t)a->map & (a->map_dtype == TODGPU_PACKED_F32 ? 15 : 7)) != 0)
-      return fail(TODGPU_EINVAL, "packed map must be aligned to its record size");
+    if (packed && ((uintptr_t)a->map & (a->map_dtype == TODGPU_PACKED_BF16 ? 7 : 15)) != 0)
+      return fail(TODGPU_EINVAL, "packed map must be aligned to 16 bytes (8 for bfloat16 records)");
     if (a->tod_stride < a->B) return fail(TODGPU_ESHAPE, "tod_stride < B");
     if (a->B > 0 && a->S > 0 && (!a->map || !a->tod || !a->beam_vals))
       return fail(TODGPU_EINVAL, "NULL map, tod or beam_vals");
@@ -650,13 +666,21 @@ extern "C" int todgpu_pack_map(const void* planar, int32_t planar_dtype, int64_t
   if (!planar || !out) return fail(TODGPU_EINVAL, "NULL pointer");
   if (C < 1 || C > 4 || N < 0 || stride < N) return fail(TODGPU_ESHAPE, "bad map shape");
   if (planar_dtype != TODGPU_F32 && planar_dtype != TODGPU_F64) return fail(TODGPU_EDTYPE, "planar dtype");
-  if (packed_dtype != TODGPU_PACKED_F32 && packed_dtype != TODGPU_PACKED_BF16)
+  if (packed_dtype != TODGPU_PACKED_F32 && packed_dtype != TODGPU_PACKED_BF16 && packed_dtype != TODGPU_PACKED_F64)
     return fail(TODGPU_EDTYPE, "packed dtype");
-  if (((uintptr_t)out & (packed_dtype == TODGPU_PACKED_F32 ? 15 : 7)) != 0)
-    return fail(TODGPU_EINVAL, "packed map must be aligned to its record size");
+  if (((uintptr_t)out & (packed_dtype == TODGPU_PACKED_BF16 ? 7 : 15)) != 0)
+    return fail(TODGPU_EINVAL, "packed map must be aligned to 16 bytes (8 for bfloat16 records)");
   if (N == 0) return TODGPU_OK;
   cudaStream_t s = static_cast<cudaStream_t>(stream);
   const int g = grid_for(N, 256);
+  if (packed_dtype == TODGPU_PACKED_F64) {
+    if (planar_dtype == TODGPU_F32)
+      pack_map_f64_kernel<float><<<g, 256, 0, s>>>(static_cast<const float*>(planar), (int)C, N, stride, out);
+    else
+      pack_map_f64_kernel<double><<<g, 256, 0, s>>>(static_cast<const double*>(planar), (int)C, N, stride, out);
+    cudaError_t e = cudaGetLastError();
+    return e == cudaSuccess ? TODGPU_OK : cuda_fail(e, "pack_map_f64_kernel launch");
+  }
   const bool bf = packed_dtype == TODGPU_PACKED_BF16;
   if (planar_dtype == TODGPU_F32) {
     if (bf)

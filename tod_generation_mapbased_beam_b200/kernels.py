@@ -139,8 +139,10 @@ def make_args(interp, nside, B, S, C, c_q, c_u, params, pdt, bore_phi, beam, mp,
 
 
 class PackedMap:
-    """A map in the precision form's layout: one record of 4 components per
-    pixel (float32, 16 B, or bfloat16, 8 B), built by :func:`pack_map`."""
+    """A map with one record of 4 components per pixel: float32 (16 B) or
+    bfloat16 (8 B) for the precision form, float64 (32 B) for the float64
+    path with a pixel's components side by side (same results as the planar
+    float64 map).  Built by :func:`pack_map`."""
 
     def __init__(self, data: torch.Tensor, C: int, kind: str):
         self.data = data
@@ -149,29 +151,33 @@ class PackedMap:
 
     @property
     def map_dtype(self):
-        return _native.PACKED_F32 if self.kind == "f32" else _native.PACKED_BF16
+        return {"f32": _native.PACKED_F32, "bf16": _native.PACKED_BF16, "f64": _native.PACKED_F64}[self.kind]
 
     @property
     def npix(self):
         return self.data.shape[0]
 
+    @property
+    def device(self):
+        return self.data.device
+
 
 def pack_map(mp_stacked, kind="f32"):
     """Pack a planar (C, N) map (numpy or torch, float32/float64, C <= 4) into
-    the precision form's per-pixel records on the GPU (todgpu_pack_map)."""
-    if kind not in ("f32", "bf16"):
-        raise ValueError("kind must be 'f32' or 'bf16'")
+    per-pixel records on the GPU (todgpu_pack_map): "f32" or "bf16" for the
+    precision form, "f64" for the float64 path."""
+    if kind not in ("f32", "bf16", "f64"):
+        raise ValueError("kind must be 'f32', 'bf16' or 'f64'")
     mp = _map_tensor(mp_stacked)
     C, N = mp.shape
     if C > 4:
         raise ValueError("at most 4 components per record")
-    if kind == "f32":
-        out = torch.empty((N, 4), dtype=torch.float32, device=mp.device)
-    else:
-        out = torch.empty((N, 4), dtype=torch.bfloat16, device=mp.device)
+    dt = {"f32": torch.float32, "bf16": torch.bfloat16, "f64": torch.float64}[kind]
+    out = torch.empty((N, 4), dtype=dt, device=mp.device)
     _native.check(_native.lib().todgpu_pack_map(
         mp.data_ptr(), _native.F32 if mp.dtype == torch.float32 else _native.F64, C, N, mp.stride(0),
-        _native.PACKED_F32 if kind == "f32" else _native.PACKED_BF16, out.data_ptr(), stream_handle()))
+        {"f32": _native.PACKED_F32, "bf16": _native.PACKED_BF16, "f64": _native.PACKED_F64}[kind], out.data_ptr(),
+        stream_handle()))
     return PackedMap(out, C, kind)
 
 

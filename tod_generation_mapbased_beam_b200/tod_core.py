@@ -16,6 +16,8 @@ Differences, all additive:
 * without ``data["mp_stacked"]`` the ``mp`` component list is stacked and
   uploaded (the reference falls back to a healpy path there, which needs
   healpy; the result is the same gather);
+* a float64 map is kept on the device as float64 records {I, Q, U, 0} (one
+  memory sector per pixel; the same TOD bit for bit);
 * ``return_device=True`` returns the (C, B) float64 CUDA accumulator instead
   of the float32 host dict.
 """
@@ -29,7 +31,7 @@ import torch
 
 from . import _native
 from ._device import is_tensor, require_cuda
-from .kernels import beam_center_angles, boresight_phi_host, gather_accum, gather_accum_angles
+from .kernels import beam_center_angles, boresight_phi_host, gather_accum, gather_accum_angles, pack_map
 from .tod_rotations import _rotation_params, precompute_rotation_vector_batch  # noqa: F401
 
 _INTERP = {"bilinear": _native.BILINEAR, "nearest": _native.NEAREST}
@@ -90,6 +92,30 @@ def stacked_map(data, mp):
     return t
 
 
+_packed = {}  # id(planar device map) -> (PackedMap, weak reference to the planar map)
+
+
+def device_map(data, mp):
+    """The entry's device map in the layout the kernels read fastest: a
+    float64 map of up to 4 components as float64 records {I, Q, U, 0}
+    (packed once and cached; the TOD is the same bit for bit), a float32 map
+    planar (its float32 products are part of the reference's result)."""
+    t = stacked_map(data, mp)
+    if t.dtype != torch.float64 or t.shape[0] > 4:
+        return t
+    key = id(t)
+    hit = _packed.get(key)
+    if hit is not None and hit[1]() is t:
+        return hit[0]
+    pm = pack_map(t, "f64")
+    try:
+        ref = weakref.ref(t, lambda _r, k=key: _packed.pop(k, None))
+    except TypeError:
+        return pm
+    _packed[key] = (pm, ref)
+    return pm
+
+
 def component_slots(comp_indices):
     """(c_q, c_u): positions of Stokes Q (1) and U (2) in comp_indices, or -1."""
     c_q = c_u = -1
@@ -120,7 +146,7 @@ def beam_tod_batch(nside, mp, data, rot_vecs, phi_b, theta_b, psis_b, interp_mod
     bore_phi = boresight_phi_host(params[3]) if (c_q >= 0 and c_u >= 0) else None
     vec = _cache.get(vec_orig, torch.float32)
     bv = _cache.get(beam_vals, torch.float32)
-    mpd = stacked_map(data, mp)
+    mpd = device_map(data, mp)
     tod = torch.zeros((C, B), dtype=torch.float64, device=mpd.device)
     gather_accum(_INTERP[interp_mode], vec, *params, nside, mpd, bv, B, S, tod, c_q, c_u,
                  bore_phi=bore_phi if bore_phi is not None else np.zeros(B, np.float32))
@@ -155,7 +181,7 @@ def beam_tod_angles(nside, data, theta_b, phi_b, psi_b, interp_mode="bilinear", 
         center = beam_center_angles(data["ra"], data["dec"])
     vec = _cache.get(data["vec_orig"], torch.float64)
     bv = _cache.get(data["beam_vals"], torch.float32)
-    mpd = stacked_map(data, mp)
+    mpd = device_map(data, mp)
     tod = torch.zeros((C, B), dtype=torch.float64, device=mpd.device)
     gather_accum_angles(_INTERP[interp_mode], vec, theta_b, phi_b, psi_b, center[0], center[1], nside,
                         mpd, bv, tod, c_q, c_u)

@@ -10,8 +10,8 @@ at pointings uniform on the sphere (theta, phi) and in roll psi, trains a
 :class:`~tod_generation_mapbased_beam_b200.tailnet.TailNet` on them, judges it
 on held-out pointings of a scan against the plain tail sum, and then adds its
 prediction in place of the tail.  The plain tail sum stays available as the
-fallback (``tail="plain"``; ``tail="auto"`` chooses it when the judged error
-exceeds the budget).
+fallback (``tail="plain"``; ``tail="auto"`` chooses it when the held-out error
+measured by :meth:`LearnedTailTOD.judge` exceeds the budget).
 
 The reference reduces a tail by k-means clustering instead
 (beam_cluster.py:215-397, hybrid mode); the main/tail split rule of that mode
@@ -165,7 +165,7 @@ class LearnedTailTOD:
 
     def tod(self, theta, phi, psi, tail="auto"):
         """(3, B) float64 I/Q/U TOD: main lobe plus the tail from the network
-        ("learned"), the plain method ("plain"), the judged choice ("auto"),
+        ("learned"), the plain method ("plain"), the choice made by judge() ("auto"),
         or none ("none")."""
         if tail == "auto":
             if self.judged is None:

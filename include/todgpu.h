@@ -234,6 +234,15 @@ int todgpu_alm2map(int64_t nside, int32_t lmax, const void *alm, void *workspace
  * never written in practice.  Time it with CUDA events on `stream`. */
 int todgpu_fp64_probe(int64_t blocks, int32_t iters, double *sink, double *flops, void *stream);
 
+/* L2 bandwidth probe (measurement helper; no counterpart in the reference):
+ * `blocks` CTAs of 256 threads read the device buffer `buf` (16-byte aligned;
+ * size it to fit in L2) `iters` times with 16-byte loads that bypass L1;
+ * *bytes_read receives the bytes the launch reads (host).  `sink` is a device
+ * buffer of `blocks` unsigned ints, never written in practice.  Time it with
+ * CUDA events on `stream`. */
+int todgpu_l2_probe(const void *buf, size_t bytes, int32_t iters, unsigned *sink, int64_t blocks, double *bytes_read,
+                    void *stream);
+
 /*
  * Learned far-sidelobe tail (no counterpart in the reference, whose only
  * tail reduction is the k-means clustering of beam_cluster.py:215-397; the

@@ -134,6 +134,8 @@ def _declare(lib):
     lib.todgpu_alm2map.restype = ctypes.c_int
     lib.todgpu_fp64_probe.argtypes = [_i64, _i32, _p, ctypes.POINTER(ctypes.c_double), _p]
     lib.todgpu_fp64_probe.restype = ctypes.c_int
+    lib.todgpu_l2_probe.argtypes = [_p, ctypes.c_size_t, _i32, _p, _i64, ctypes.POINTER(ctypes.c_double), _p]
+    lib.todgpu_l2_probe.restype = ctypes.c_int
     mp = ctypes.POINTER(MlpDesc)
     lib.todgpu_mlp_param_count.argtypes = [mp]
     lib.todgpu_mlp_param_count.restype = _i64
@@ -226,6 +228,7 @@ def exported_symbols():
         "todgpu_alm2map_workspace_bytes",
         "todgpu_alm2map",
         "todgpu_fp64_probe",
+        "todgpu_l2_probe",
         "todgpu_mlp_set_forward_path",
         "todgpu_mlp_wait_timeouts",
         "todgpu_mlp_tcgen05_launches",

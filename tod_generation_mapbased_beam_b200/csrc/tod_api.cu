@@ -661,6 +661,33 @@ extern "C" int todgpu_fp64_probe(int64_t blocks, int32_t iters, double* sink, do
   return TODGPU_OK;
 }
 
+// L2 bandwidth probe: every thread streams 16-byte loads that bypass L1
+// (ld.global.cg) over a buffer that fits in L2, `iters` passes.
+__global__ void l2_probe_kernel(const uint4* buf, long long n16, int iters, unsigned* sink) {
+  unsigned acc = 0;
+  const long long stride = (long long)gridDim.x * blockDim.x;
+  for (int it = 0; it < iters; ++it)
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n16; i += stride) {
+      const uint4 v = __ldcg(buf + i);
+      acc ^= v.x ^ v.y ^ v.z ^ v.w;
+    }
+  if (acc == 0x9e3779b9u) sink[blockIdx.x] = acc;  // keeps the loads; practically never true
+}
+
+extern "C" int todgpu_l2_probe(const void* buf, size_t bytes, int32_t iters, unsigned* sink, int64_t blocks,
+                               double* bytes_read, void* stream) {
+  if (!buf || !sink || !bytes_read || bytes < 16 || iters < 1 || blocks < 1)
+    return fail(TODGPU_EINVAL, "bad probe arguments");
+  if (((uintptr_t)buf & 15) != 0) return fail(TODGPU_EINVAL, "buffer must be 16-byte aligned");
+  const long long n16 = (long long)(bytes / 16);
+  l2_probe_kernel<<<(unsigned)blocks, 256, 0, static_cast<cudaStream_t>(stream)>>>(static_cast<const uint4*>(buf),
+                                                                                   n16, iters, sink);
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return cuda_fail(e, "l2_probe_kernel launch");
+  *bytes_read = 16.0 * (double)n16 * (double)iters;
+  return TODGPU_OK;
+}
+
 extern "C" int todgpu_pack_map(const void* planar, int32_t planar_dtype, int64_t C, int64_t N, int64_t stride,
                                int32_t packed_dtype, void* out, void* stream) {
   if (!planar || !out) return fail(TODGPU_EINVAL, "NULL pointer");

@@ -951,14 +951,38 @@ __device__ void run_samples(const KArgs& a, long long t_begin, long long t_end, 
     w.ir_lo = 0;
     w.ir_lo32 = 0;
   }
+  // Angles mode: one thread derives each sample's rotation and boresight, one
+  // sample ahead, into a double-buffered shared slot instead of every thread
+  // computing the same values -- the last thread, which has the fewest beam
+  // pixels when S is not a multiple of the CTA size.  Other modes load their
+  // per-sample parameters in every thread (a few cached loads).
+  constexpr bool kShareRot = (PM == kAngles);
+  constexpr int kRotThread = NT - 1;
+  __shared__ SampleRot s_rot[2];
+  __shared__ Bore s_bo[2];
+  if constexpr (kShareRot) {
+    if (threadIdx.x == kRotThread && t_begin < t_end) {
+      const long long b0 = t_begin * tile;
+      s_rot[0] = load_rot<PM>(a, b0);
+      if (HAS_QU) load_boresight<PM>(a, s_rot[0], b0, s_bo[0].z, s_bo[0].sth, s_bo[0].phi);
+    }
+  }
+  int slot = 0;
   unsigned long long nerr = 0;
   long long prev = -1;
   for (long long t = t_begin; t < t_end; t += t_step)
   for (long long b = t * tile, b_stop = min(a.B, (t + 1) * tile); b < b_stop; ++b) {
-    const SampleRot rot = load_rot<PM>(a, b);
+    SampleRot rot;
     Bore bo{0.0, 0.0, 0.0};
-    if (HAS_QU) load_boresight<PM>(a, rot, b, bo.z, bo.sth, bo.phi);
-    __syncthreads();  // previous sample is done with the table and its partial sums
+    if constexpr (!kShareRot) {
+      rot = load_rot<PM>(a, b);
+      if (HAS_QU) load_boresight<PM>(a, rot, b, bo.z, bo.sth, bo.phi);
+    }
+    __syncthreads();  // previous sample is done with the table, its partial sums and its slot
+    if constexpr (kShareRot) {
+      rot = s_rot[slot];
+      if (HAS_QU) bo = s_bo[slot];
+    }
     if (prev >= 0 && threadIdx.x == 0) flush_sample<NW>(a, s_red, prev);
     if (use_tab) {
       if (threadIdx.x < kSetupThreads) {
@@ -1047,6 +1071,22 @@ __device__ void run_samples(const KArgs& a, long long t_begin, long long t_end, 
       if (c >= a.C) break;
       const double v = warp_sum(acc.total(c));
       if (lane == 0) s_red[warp * 4 + c] = v;
+    }
+    if constexpr (kShareRot) {
+      // the next sample's rotation into the other slot (read after the next barrier)
+      if (threadIdx.x == kRotThread) {
+        long long bn = b + 1, tn = t;
+        if (bn >= b_stop) {
+          tn = t + t_step;
+          bn = tn * tile;
+        }
+        if (tn < t_end && bn < a.B) {
+          s_rot[slot ^ 1] = load_rot<PM>(a, bn);
+          if (HAS_QU) load_boresight<PM>(a, s_rot[slot ^ 1], bn, s_bo[slot ^ 1].z, s_bo[slot ^ 1].sth,
+                                         s_bo[slot ^ 1].phi);
+        }
+      }
+      slot ^= 1;
     }
     prev = b;
   }

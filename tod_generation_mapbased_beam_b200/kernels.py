@@ -21,6 +21,7 @@ parameters give an all-float64 computation.
 from __future__ import annotations
 
 import ctypes
+import weakref
 
 import numpy as np
 import torch
@@ -61,12 +62,33 @@ _RING_TABLES = {}
 _REACH_STEP = 1e-4  # ring tables are built for reaches rounded up to this step [rad]
 
 
+_REACH = {}  # (tensor identity, version, nside) -> (reach, weak reference to the tensor)
+
+
 def beam_reach(vec_orig, nside):
     """Angular radius [rad] that every stencil neighbour of the rotated beam
     stays within around the rotated beam centre: the beam's radius about its
     mean direction plus 3/nside (stencil reach) plus float32 slack.  The
     kernel derives the same bound from the beam on the device and uses the
-    ring table's spin-2 slots only if the table covers it."""
+    ring table's spin-2 slots only if the table covers it.  For a CUDA tensor
+    the value is remembered (until the tensor changes or is freed), so repeated
+    calls do not copy the beam back to the host."""
+    key = None
+    if is_tensor(vec_orig):
+        key = (id(vec_orig), vec_orig.data_ptr(), vec_orig._version, tuple(vec_orig.shape), int(nside))
+        hit = _REACH.get(key)
+        if hit is not None and hit[1]() is vec_orig:
+            return hit[0]
+    r = _beam_reach(vec_orig, nside)
+    if key is not None:
+        try:
+            _REACH[key] = (r, weakref.ref(vec_orig, lambda _r, k=key: _REACH.pop(k, None)))
+        except TypeError:
+            pass
+    return r
+
+
+def _beam_reach(vec_orig, nside):
     v = vec_orig.detach().cpu().numpy() if is_tensor(vec_orig) else np.asarray(vec_orig)
     v = np.asarray(v, np.float64).reshape(-1, 3)
     if v.shape[0] == 0:

@@ -592,7 +592,7 @@ def run_precision(args, dist, sky):
     idx = torch.from_numpy(np.linspace(0, B - 1, 4096).astype(np.int64)).to(dev)
     out, subs = {}, {}
     for kind in ("f64", "f32", "bf16"):
-        mp = sky if kind == "f64" else pack_map(sky, kind)
+        mp = pack_map(sky, kind)
         tod = torch.zeros((3, B), dtype=torch.float64, device=dev)
 
         def launch():
@@ -603,7 +603,8 @@ def run_precision(args, dist, sky):
         ms = dist.max(_evt_ms(launch, stream))
         subs[kind] = tod[:, idx].cpu().numpy()
         out[kind] = {"value": B * dist.world / (ms / 1e3), "ms_per_step": ms,
-                     "map": {"f64": "planar float64", "f32": "packed f32 records (16 B/pixel)",
+                     "map": {"f64": "packed f64 records (32 B/pixel; TOD bit-identical to the planar "
+                                    "float64 map)", "f32": "packed f32 records (16 B/pixel)",
                              "bf16": "packed bf16 records (8 B/pixel)"}[kind]}
         del tod, mp
     for kind in ("f32", "bf16"):

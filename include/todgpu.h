@@ -159,6 +159,19 @@ int todgpu_gather_accum_batched(const todgpu_gather_args *jobs, int32_t njobs, i
  * reference. */
 int todgpu_gather_accum_static(const todgpu_gather_args *args, void *stream);
 
+/* Pointing preparation on the device (tod_rotations.py:219-333 with the roll
+ * psi_b - beta of gridint.py:281, all in float64): for B samples (theta, phi,
+ * psi) (angles_dtype TODGPU_F32 or TODGPU_F64) and the beam centre
+ * (center_phi, center_theta), the rotation parameters axes (B, 3), cos_a,
+ * sin_a, ax_pts (B, 3), cos_p, sin_p -- float64 device arrays -- exactly as
+ * the TODGPU_ANGLES mode derives them inside the gather; a gather with
+ * params_dtype = TODGPU_F64 on them gives the same TOD bit for bit.
+ * Replaces the host step precompute_rotation_vector_batch + _rotation_params
+ * for callers that keep the rotation on the GPU. */
+int todgpu_pointing_params(const void *theta, const void *phi, const void *psi, int32_t angles_dtype, int64_t B,
+                           double center_phi, double center_theta, double *axes, double *cos_a, double *sin_a,
+                           double *ax_pts, double *cos_p, double *sin_p, void *stream);
+
 /* Per-(b, s) bilinear stencil of the fused path: pix (4, B*S) int64 and
  * wgt (4, B*S) float64 with n = b*S + s.  Replaces the split reference path
  * tod_rotations._rodrigues_jit (tod_rotations.py:33-80) + vec2ang +

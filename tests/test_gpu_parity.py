@@ -224,7 +224,7 @@ def test_device_pointing_matches_fp64_ideal_oracle(mode, angles_dtype):
     tod = torch.zeros((3, B), dtype=torch.float64, device="cuda")
     # the beam is centred on the beam-frame pole: (phi_c, theta_c) = (0, 0)
     gather_accum_angles(interp, beam.vec_orig.astype(np.float64), theta, phi, psi, 0.0, 0.0, nside,
-                        mp, beam.beam_vals, tod, 1, 2)
+                        mp, beam.beam_vals, tod, 1, 2, precompute=False)
     rot, beta = oracle.rotation_vectors_f64(0.0, 0.0, phi.astype(np.float64), theta.astype(np.float64))
     params = oracle.rotation_params_f64(rot, phi, theta, psi.astype(np.float64) - beta)
     cpu = np.zeros((3, B))
@@ -336,3 +336,44 @@ def test_packed_f64_map_bit_identical_device_pointing(mode):
                             beam.beam_vals, tod, 1, 2)
         outs.append(tod.cpu().numpy())
     assert np.array_equal(outs[0], outs[1])
+
+
+@pytest.mark.parametrize("angles_dtype", [np.float32, np.float64])
+def test_pointing_params_match_oracle(angles_dtype):
+    """Device pointing preparation against the float64 oracle of
+    tod_rotations.py:219-333 (beam centre off the pole, so the Rodrigues
+    vectors and beta are non-trivial)."""
+    from tod_generation_mapbased_beam_b200 import workloads as W
+    from tod_generation_mapbased_beam_b200.kernels import pointing_params
+
+    th, ph, ps = (x.astype(angles_dtype) for x in W.spin_scan(5000, 30.0, phi0=0.7))
+    cphi, cth = 0.4, 0.02
+    got = [t.cpu().numpy() for t in pointing_params(th, ph, ps, cphi, cth)]
+    rot, beta = oracle.rotation_vectors_f64(cphi, cth, ph.astype(np.float64), th.astype(np.float64))
+    ref = oracle.rotation_params_f64(rot, ph, th, ps.astype(np.float64) - beta)
+    for g, r in zip(got, ref):
+        assert g.shape == np.shape(r)
+        assert np.abs(g - r).max() <= 1e-13
+
+
+@pytest.mark.parametrize("mode", ["bilinear", "nearest"])
+@pytest.mark.parametrize("angles_dtype", [np.float32, np.float64])
+def test_precomputed_pointing_bit_identical_to_angles_mode(mode, angles_dtype):
+    """The prepared float64 parameters through the gather's float64 mode give
+    the angles-mode TOD bit for bit (planar and packed float64 maps)."""
+    from tod_generation_mapbased_beam_b200 import _native
+    from tod_generation_mapbased_beam_b200 import workloads as W
+    from tod_generation_mapbased_beam_b200.kernels import gather_accum_angles, pack_map
+
+    beam = W.pole_gaussian_beam(60.0, 512, 0.99, search_fwhm=1.5)
+    th, ph, ps = (x.astype(angles_dtype) for x in W.spin_scan(4000, 50.0, phi0=2.1))
+    sky = W.white_sky(256, 9)
+    interp = _native.BILINEAR if mode == "bilinear" else _native.NEAREST
+    for m in (sky, pack_map(sky, "f64")):
+        outs = []
+        for pre in (False, True):
+            tod = torch.zeros((3, len(th)), dtype=torch.float64, device="cuda")
+            gather_accum_angles(interp, beam.vec_orig.astype(np.float64), th, ph, ps, 0.0, 0.0, 256, m,
+                                beam.beam_vals, tod, 1, 2, precompute=pre)
+            outs.append(tod.cpu().numpy())
+        assert np.array_equal(outs[0], outs[1])

@@ -134,6 +134,8 @@ def _declare(lib):
     lib.todgpu_alm2map.restype = ctypes.c_int
     lib.todgpu_fp64_probe.argtypes = [_i64, _i32, _p, ctypes.POINTER(ctypes.c_double), _p]
     lib.todgpu_fp64_probe.restype = ctypes.c_int
+    lib.todgpu_pointing_params.argtypes = [_p, _p, _p, _i32, _i64, ctypes.c_double, ctypes.c_double] + [_p] * 6 + [_p]
+    lib.todgpu_pointing_params.restype = ctypes.c_int
     lib.todgpu_l2_probe.argtypes = [_p, ctypes.c_size_t, _i32, _p, _i64, ctypes.POINTER(ctypes.c_double), _p]
     lib.todgpu_l2_probe.restype = ctypes.c_int
     mp = ctypes.POINTER(MlpDesc)
@@ -229,6 +231,7 @@ def exported_symbols():
         "todgpu_alm2map",
         "todgpu_fp64_probe",
         "todgpu_l2_probe",
+        "todgpu_pointing_params",
         "todgpu_mlp_set_forward_path",
         "todgpu_mlp_wait_timeouts",
         "todgpu_mlp_tcgen05_launches",

@@ -3,7 +3,10 @@
 :class:`DetectorBatch` holds, on the GPU, every detector's beam (vectors and
 weights), its scan angles and its (C, n) float64 output, and runs them all
 with one ``todgpu_gather_accum_batched`` launch -- the rotation of each sample
-derived on the device from its angles (FP64).  The launch is captured in a
+derived on the device from its angles (FP64): by default first into float64
+parameter buffers, one ``todgpu_pointing_params`` launch per detector, which
+the batched gather then reads (``precompute=False``: inside the gather, same
+result bit for bit).  The launches are captured in a
 CUDA graph on first use and replayed afterwards (``graph=True``), and its
 tile size (samples per work tile) is chosen by :mod:`autotune` unless given.
 
@@ -21,12 +24,13 @@ import torch
 
 from . import _native
 from ._device import require_cuda, stream_handle, to_device
-from .kernels import PackedMap, _map_tensor, _ncomp, _set_map, beam_reach, ring_table
+from .kernels import (PackedMap, _map_tensor, _ncomp, _set_map, beam_reach, pointing_buffers, pointing_params,
+                      ring_table)
 
 
 class DetectorBatch:
     def __init__(self, nside, mp, detectors, comp_indices=(0, 1, 2), interp_mode="bilinear",
-                 tile=None, graph=True, tables=True):
+                 tile=None, graph=True, tables=True, precompute=True):
         require_cuda()
         if interp_mode not in ("bilinear", "nearest"):
             raise ValueError(f"interp_mode {interp_mode!r} not available on main branch; "
@@ -53,6 +57,7 @@ class DetectorBatch:
             self.centers.append(tuple(d.get("center", (0.0, 0.0))))
             if vec.shape[0]:
                 reach = max(reach, beam_reach(vec, self.nside))
+        self.rot = [pointing_buffers(a[0].shape[0], dev) for a in self.angles] if precompute else None
         self.table = ring_table(self.nside, reach, dev) if (tables and reach > 0) else None
         self.flags = 0 if tables else _native.FLAG_NO_TABLES
         self._args = self._make_args()
@@ -80,12 +85,16 @@ class DetectorBatch:
             a.S = vec.shape[0]
             a.C = self.C
             a.c_q, a.c_u = self.c_q, self.c_u
-            a.params_dtype = _native.ANGLES
             _set_map(a, self.map)
             a.vec_orig = vec.data_ptr()
-            a.theta, a.phi, a.psi = (t.data_ptr() for t in ang)
-            a.angles_dtype = _native.F32
-            a.center_phi, a.center_theta = cen
+            if self.rot is not None:
+                a.params_dtype = _native.F64
+                (a.axes, a.cos_a, a.sin_a, a.ax_pts, a.cos_p, a.sin_p) = (t.data_ptr() for t in self.rot[j])
+            else:
+                a.params_dtype = _native.ANGLES
+                a.theta, a.phi, a.psi = (t.data_ptr() for t in ang)
+                a.angles_dtype = _native.F32
+                a.center_phi, a.center_theta = cen
             a.beam_vals = bv.data_ptr()
             a.tod = out.data_ptr()
             a.tod_stride = out.stride(0)
@@ -111,6 +120,9 @@ class DetectorBatch:
         """Zero the outputs and launch once on the current stream (no graph)."""
         for o in self.out:
             o.zero_()
+        if self.rot is not None:
+            for ang, rot, cen in zip(self.angles, self.rot, self.centers):
+                pointing_params(*ang, cen[0], cen[1], out=rot)
         t = int(tile or self.tile or 256)
         _native.check(_native.lib().todgpu_gather_accum_batched(self._args, len(self._args), t,
                                                                 stream_handle()))

@@ -661,6 +661,28 @@ extern "C" int todgpu_fp64_probe(int64_t blocks, int32_t iters, double* sink, do
   return TODGPU_OK;
 }
 
+// Pointing preparation on the device: per sample the float64 rotation
+// parameters of tod_rotations.py:306-333 derived from the angles exactly as
+// the gather kernel's angles mode derives them (rot_from_angles), written
+// structure-of-arrays for the float64-parameter mode.
+__global__ void pointing_params_kernel(const KArgs k, double* axes, double* cos_a, double* sin_a, double* pts,
+                                       double* cos_p, double* sin_p) {
+  for (long long b = blockIdx.x * (long long)blockDim.x + threadIdx.x; b < k.B;
+       b += (long long)gridDim.x * blockDim.x) {
+    const SampleRot r = rot_from_angles(k, b);
+    axes[3 * b] = r.kx;
+    axes[3 * b + 1] = r.ky;
+    axes[3 * b + 2] = r.kz;
+    cos_a[b] = r.ca;
+    sin_a[b] = r.sa;
+    pts[3 * b] = r.px;
+    pts[3 * b + 1] = r.py;
+    pts[3 * b + 2] = r.pz;
+    cos_p[b] = r.cp;
+    sin_p[b] = r.sp;
+  }
+}
+
 // L2 bandwidth probe: every thread streams 16-byte loads that bypass L1
 // (ld.global.cg) over a buffer that fits in L2, `iters` passes.
 __global__ void l2_probe_kernel(const uint4* buf, long long n16, int iters, unsigned* sink) {
@@ -672,6 +694,29 @@ __global__ void l2_probe_kernel(const uint4* buf, long long n16, int iters, unsi
       acc ^= v.x ^ v.y ^ v.z ^ v.w;
     }
   if (acc == 0x9e3779b9u) sink[blockIdx.x] = acc;  // keeps the loads; practically never true
+}
+
+extern "C" int todgpu_pointing_params(const void* theta, const void* phi, const void* psi, int32_t angles_dtype,
+                                      int64_t B, double center_phi, double center_theta, double* axes, double* cos_a,
+                                      double* sin_a, double* pts, double* cos_p, double* sin_p, void* stream) {
+  if (B < 0) return fail(TODGPU_ESHAPE, "B must be >= 0");
+  if (B == 0) return TODGPU_OK;
+  if (!theta || !phi || !psi || !axes || !cos_a || !sin_a || !pts || !cos_p || !sin_p)
+    return fail(TODGPU_EINVAL, "NULL pointer");
+  if (angles_dtype != TODGPU_F32 && angles_dtype != TODGPU_F64) return fail(TODGPU_EDTYPE, "bad angles_dtype");
+  todgpu_gather_args a{};
+  a.B = B;
+  a.theta = theta;
+  a.phi = phi;
+  a.psi = psi;
+  a.angles_dtype = angles_dtype;
+  a.center_phi = center_phi;
+  a.center_theta = center_theta;
+  const KArgs k = make_kargs(&a);
+  pointing_params_kernel<<<grid_for(B, 256), 256, 0, static_cast<cudaStream_t>(stream)>>>(k, axes, cos_a, sin_a, pts,
+                                                                                        cos_p, sin_p);
+  cudaError_t e = cudaGetLastError();
+  return e == cudaSuccess ? TODGPU_OK : cuda_fail(e, "pointing_params_kernel launch");
 }
 
 extern "C" int todgpu_l2_probe(const void* buf, size_t bytes, int32_t iters, unsigned* sink, int64_t blocks,

@@ -306,25 +306,72 @@ def beam_center_angles(ra, dec, center_idx=None):
     return float(ra[center_idx]), float(np.pi / 2 - dec[center_idx])
 
 
-def gather_accum_angles(interp, vec_orig, theta, phi, psi, center_phi, center_theta, nside,
-                        mp_stacked, beam_vals, tod, c_q=-1, c_u=-1, err_count=None, flags=0,
-                        static_table=False):
-    """One fused launch with the pointing given as angles: every CTA derives
-    the sample's rotation on the device in float64 from (theta, phi, psi) and
-    the beam centre (no float32 parameter rounding).  ``tod`` must be a float64
-    (C, B) CUDA tensor; it is accumulated in place.  ``theta, phi, psi`` may be
-    float32 or float64 (a float32 scan is widened exactly on the device)."""
-    require_cuda()
-    vec = to_device(vec_orig, np.float64).reshape(-1, 3)
-    S = vec.shape[0]
+def _angles_on_device(theta, phi, psi):
     adt = dtype_of(theta)
     adt = np.float32 if adt == np.dtype(np.float32) else np.float64
     th = to_device(theta, adt).reshape(-1)
     ph = to_device(phi, adt).reshape(-1)
     ps = to_device(psi, adt).reshape(-1)
-    B = th.shape[0]
-    if ph.shape[0] != B or ps.shape[0] != B:
+    if ph.shape[0] != th.shape[0] or ps.shape[0] != th.shape[0]:
         raise ValueError("theta, phi and psi must have the same length")
+    return adt, th, ph, ps
+
+
+def pointing_buffers(B, device):
+    """Uninitialised float64 (axes (B, 3), cos_a, sin_a, ax_pts (B, 3), cos_p,
+    sin_p) for :func:`pointing_params`."""
+    axes = torch.empty((B, 3), dtype=torch.float64, device=device)
+    pts = torch.empty((B, 3), dtype=torch.float64, device=device)
+    cos_a, sin_a, cos_p, sin_p = (torch.empty(B, dtype=torch.float64, device=device) for _ in range(4))
+    return axes, cos_a, sin_a, pts, cos_p, sin_p
+
+
+def pointing_params(theta, phi, psi, center_phi, center_theta, out=None):
+    """Float64 rotation parameters (axes (B, 3), cos_a, sin_a, ax_pts (B, 3),
+    cos_p, sin_p) of every sample, derived on the device from the pointing
+    angles and the beam centre -- the reference's
+    precompute_rotation_vector_batch + _rotation_params
+    (tod_rotations.py:219-333) in float64, one thread per sample.  A float64
+    gather on them equals the angles-mode gather bit for bit.  ``out``: six
+    contiguous float64 CUDA tensors of at least B samples to fill (e.g. from
+    :func:`pointing_buffers`); returned as given."""
+    require_cuda()
+    adt, th, ph, ps = _angles_on_device(theta, phi, psi)
+    B = th.shape[0]
+    if out is None:
+        out = pointing_buffers(B, th.device)
+    elif len(out) != 6 or any(not (is_tensor(t) and t.is_cuda and t.dtype == torch.float64 and t.is_contiguous()
+                                   and t.shape[0] >= B) for t in out):
+        raise ValueError("out must be six contiguous float64 CUDA tensors of at least B samples")
+    axes, cos_a, sin_a, pts, cos_p, sin_p = out
+    _native.check(_native.lib().todgpu_pointing_params(
+        th.data_ptr(), ph.data_ptr(), ps.data_ptr(), _native.F32 if adt == np.float32 else _native.F64, B,
+        float(center_phi), float(center_theta), axes.data_ptr(), cos_a.data_ptr(), sin_a.data_ptr(),
+        pts.data_ptr(), cos_p.data_ptr(), sin_p.data_ptr(), stream_handle()))
+    return out
+
+
+def gather_accum_angles(interp, vec_orig, theta, phi, psi, center_phi, center_theta, nside,
+                        mp_stacked, beam_vals, tod, c_q=-1, c_u=-1, err_count=None, flags=0,
+                        static_table=False, precompute=True):
+    """One fused launch with the pointing given as angles: every CTA derives
+    the sample's rotation on the device in float64 from (theta, phi, psi) and
+    the beam centre (no float32 parameter rounding).  ``tod`` must be a float64
+    (C, B) CUDA tensor; it is accumulated in place.  ``theta, phi, psi`` may be
+    float32 or float64 (a float32 scan is widened exactly on the device).
+
+    ``precompute`` (default) derives the rotations first with
+    :func:`pointing_params` (one thread per sample, 80 bytes of scratch per
+    sample) and runs the gather in its float64-parameter mode: the same TOD bit
+    for bit, with the per-sample rotation taken off the gather's critical path.
+    ``precompute=False`` (and ``static_table=True``, which allocates nothing)
+    derive the rotation inside the gather."""
+    require_cuda()
+    vec = to_device(vec_orig, np.float64).reshape(-1, 3)
+    S = vec.shape[0]
+    adt, th, ph, ps = _angles_on_device(theta, phi, psi)
+    B = th.shape[0]
+    rot = pointing_params(th, ph, ps, center_phi, center_theta) if precompute and not static_table else None
     beam = to_device(beam_vals, np.float32, (S,))
     mp = _map_tensor(mp_stacked)
     C = _ncomp(mp)
@@ -340,13 +387,17 @@ def gather_accum_angles(interp, vec_orig, theta, phi, psi, center_phi, center_th
     a.C = C
     a.c_q = int(c_q)
     a.c_u = int(c_u)
-    a.params_dtype = _native.ANGLES
     _set_map(a, mp)
     a.vec_orig = vec.data_ptr()
-    a.theta, a.phi, a.psi = th.data_ptr(), ph.data_ptr(), ps.data_ptr()
-    a.angles_dtype = _native.F32 if adt == np.float32 else _native.F64
-    a.center_phi = float(center_phi)
-    a.center_theta = float(center_theta)
+    if rot is not None:
+        a.params_dtype = _native.F64
+        (a.axes, a.cos_a, a.sin_a, a.ax_pts, a.cos_p, a.sin_p) = [t.data_ptr() for t in rot]
+    else:
+        a.params_dtype = _native.ANGLES
+        a.theta, a.phi, a.psi = th.data_ptr(), ph.data_ptr(), ps.data_ptr()
+        a.angles_dtype = _native.F32 if adt == np.float32 else _native.F64
+        a.center_phi = float(center_phi)
+        a.center_theta = float(center_theta)
     a.beam_vals = beam.data_ptr()
     a.tod = tod.data_ptr()
     a.tod_stride = tod.stride(0)

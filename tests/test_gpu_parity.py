@@ -358,18 +358,27 @@ def test_pointing_params_match_oracle(angles_dtype):
 
 @pytest.mark.parametrize("mode", ["bilinear", "nearest"])
 @pytest.mark.parametrize("angles_dtype", [np.float32, np.float64])
-def test_precomputed_pointing_bit_identical_to_angles_mode(mode, angles_dtype):
+@pytest.mark.parametrize("large", [False, True])
+def test_precomputed_pointing_bit_identical_to_angles_mode(mode, angles_dtype, large):
     """The prepared float64 parameters through the gather's float64 mode give
-    the angles-mode TOD bit for bit (planar and packed float64 maps)."""
+    the angles-mode TOD bit for bit (planar and packed float64 / float32
+    maps).  The large beam (S > 4096) takes the shared per-sample slot of the
+    float64 mode, the small one the per-thread loads."""
     from tod_generation_mapbased_beam_b200 import _native
     from tod_generation_mapbased_beam_b200 import workloads as W
     from tod_generation_mapbased_beam_b200.kernels import gather_accum_angles, pack_map
 
-    beam = W.pole_gaussian_beam(60.0, 512, 0.99, search_fwhm=1.5)
-    th, ph, ps = (x.astype(angles_dtype) for x in W.spin_scan(4000, 50.0, phi0=2.1))
+    if large:
+        beam = W.pole_gaussian_beam(30.0, 4096, 0.999, search_fwhm=2.0)
+        th, ph, ps = (x.astype(angles_dtype) for x in W.spin_scan(600, 50.0, phi0=2.1))
+        assert beam.S > 4096
+    else:
+        beam = W.pole_gaussian_beam(60.0, 512, 0.99, search_fwhm=1.5)
+        th, ph, ps = (x.astype(angles_dtype) for x in W.spin_scan(4000, 50.0, phi0=2.1))
+        assert beam.S < 4096
     sky = W.white_sky(256, 9)
     interp = _native.BILINEAR if mode == "bilinear" else _native.NEAREST
-    for m in (sky, pack_map(sky, "f64")):
+    for m in (sky, pack_map(sky, "f64"), pack_map(sky, "f32")):
         outs = []
         for pre in (False, True):
             tod = torch.zeros((3, len(th)), dtype=torch.float64, device="cuda")
@@ -377,3 +386,30 @@ def test_precomputed_pointing_bit_identical_to_angles_mode(mode, angles_dtype):
                                 beam.beam_vals, tod, 1, 2, precompute=pre)
             outs.append(tod.cpu().numpy())
         assert np.array_equal(outs[0], outs[1])
+
+
+@pytest.mark.parametrize("mode", ["bilinear", "nearest"])
+@pytest.mark.parametrize("comps", [[0, 1, 2], [0, 1]])
+def test_pipelined_drop_in_bit_identical(mode, comps, monkeypatch):
+    """beam_tod_batch over a batch larger than its chunk (host preparation on
+    the thread pool overlapping the gathers) returns exactly the one-launch
+    result, ragged last chunk included."""
+    from tod_generation_mapbased_beam_b200 import tod_rotations as R
+    from tod_generation_mapbased_beam_b200 import workloads as W
+
+    nside, B = 128, 20_011
+    beam = W.pole_gaussian_beam(90.0, 256, 0.99, search_fwhm=1.5)
+    th, ph, ps = W.spin_scan(B, 20.0, phi0=0.9)
+    rot, beta = R.precompute_rotation_vector_batch(beam.ra, beam.dec, ph, th)
+    psis = -beta + ps
+    sky = W.white_sky(nside, 3)
+    data = dict(vec_orig=beam.vec_orig, beam_vals=beam.beam_vals, comp_indices=comps,
+                mp_stacked=np.ascontiguousarray(sky[comps]), ra=beam.ra, dec=beam.dec)
+    one = tod_core.beam_tod_batch(nside, None, data, rot, ph, th, psis, interp_mode=mode, return_device=True)
+    monkeypatch.setattr(tod_core, "PIPE_CHUNK", 4096)
+    piped = tod_core.beam_tod_batch(nside, None, data, rot, ph, th, psis, interp_mode=mode, return_device=True)
+    assert torch.equal(one, piped)
+    out = tod_core.beam_tod_batch(nside, None, data, rot, ph, th, psis, interp_mode=mode)
+    assert sorted(out) == sorted(comps)
+    for i, c in enumerate(comps):
+        assert np.array_equal(out[c], one[i].to(torch.float32).cpu().numpy())

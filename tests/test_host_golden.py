@@ -34,3 +34,31 @@ def test_beam_selection_bit_exact(cut):
     db = W.compute_db_threshold_from_power(g["beam"], cut)
     assert db == g[f"db_{cut}"]
     assert np.array_equal(W.select_beam_pixels(g["beam"], cut), g[f"sel_{cut}"])
+
+
+def test_chunked_parameter_preparation_bit_exact():
+    """The pipelined drop-in prepares the float32 parameters chunk by chunk on
+    a thread pool; every chunk boundary (ragged ones included) gives the
+    whole-batch values bit for bit."""
+    from tod_generation_mapbased_beam_b200 import tod_core as TC
+    from tod_generation_mapbased_beam_b200.kernels import boresight_phi_host
+
+    beam = W.pole_gaussian_beam(30.0, 256, 0.99, search_fwhm=1.5)
+    B = 50_021
+    th, ph, ps = W.spin_scan(B, 100.0, phi0=0.3)
+    rot, beta = R.precompute_rotation_vector_batch(beam.ra, beam.dec, ph, th)
+    psis = -beta + ps
+    whole = R._rotation_params(rot, ph, th, psis)
+    bore = boresight_phi_host(whole[3])
+    for step in (1 << 12, 7_777, B):
+        parts = [TC._prep_chunk(rot, ph, th, psis, a, min(B, a + step), True) for a in range(0, B, step)]
+        fields = [[] for _ in TC._PIPE_WIDTHS]
+        for a, part in zip(range(0, B, step), parts):
+            n = min(B, a + step) - a
+            o = 0
+            for i, w in enumerate(TC._PIPE_WIDTHS):
+                fields[i].append(part[o:o + w * n])
+                o += w * n
+        got = [np.concatenate(f) for f in fields]
+        for i, ref in enumerate(list(whole) + [bore]):
+            assert np.array_equal(got[i], np.asarray(ref, np.float32).reshape(-1)), (step, i)

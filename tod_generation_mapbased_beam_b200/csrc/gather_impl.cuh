@@ -94,6 +94,9 @@ struct KArgs {
 constexpr int kParamsRef32 = 0;  // reference float32 parameter arrays
 constexpr int kParamsF64 = 1;    // float64 parameter arrays
 constexpr int kAngles = 2;       // (theta, phi, psi) + beam centre, derived on the device
+constexpr int kParamsF64Shared = 3;  // float64 parameter arrays, loaded once per CTA (large beams)
+
+__host__ __device__ constexpr bool f64_params(int pm) { return pm == kParamsF64 || pm == kParamsF64Shared; }
 
 template <int PM>
 __device__ __forceinline__ double angle_at(const KArgs& a, const void* p, long long b) {
@@ -152,7 +155,7 @@ __device__ __forceinline__ SampleRot load_rot(const KArgs& a, long long b) {
   SampleRot r;
   if constexpr (PM == kAngles) {
     r = rot_from_angles(a, b);
-  } else if constexpr (PM == kParamsF64) {
+  } else if constexpr (f64_params(PM)) {
     const double* ax = static_cast<const double*>(a.axes) + 3 * b;
     const double* pt = static_cast<const double*>(a.pts) + 3 * b;
     r.kx = ax[0];
@@ -197,7 +200,7 @@ __device__ __forceinline__ void load_boresight(const KArgs& a, const SampleRot& 
     z = clamp1(rot.pz);
     sth = sqrt(max0(1.0 - rot.pz * rot.pz));
     phi = atan2(rot.py, rot.px);
-  } else if constexpr (PM == kParamsF64) {
+  } else if constexpr (f64_params(PM)) {
     const double* pt = static_cast<const double*>(a.pts) + 3 * b;
     z = clamp1(pt[2]);
     sth = sqrt(max0(1.0 - pt[2] * pt[2]));
@@ -954,9 +957,12 @@ __device__ void run_samples(const KArgs& a, long long t_begin, long long t_end, 
   // Angles mode: one thread derives each sample's rotation and boresight, one
   // sample ahead, into a double-buffered shared slot instead of every thread
   // computing the same values -- the last thread, which has the fewest beam
-  // pixels when S is not a multiple of the CTA size.  Other modes load their
-  // per-sample parameters in every thread (a few cached loads).
-  constexpr bool kShareRot = (PM == kAngles);
+  // pixels when S is not a multiple of the CTA size.  The shared float64
+  // parameter mode (chosen by the host for large beams, where every thread's
+  // boresight atan2 costs more than one thread's serial load-and-atan2 chain)
+  // does the same with loaded parameters.  Other modes load their per-sample
+  // parameters in every thread (a few cached loads).
+  constexpr bool kShareRot = (PM == kAngles || PM == kParamsF64Shared);
   constexpr int kRotThread = NT - 1;
   __shared__ SampleRot s_rot[2];
   __shared__ Bore s_bo[2];
@@ -1164,6 +1170,10 @@ constexpr size_t kTabHeaderBytes = (sizeof(Spin2Tab) + 15) & ~size_t(15);
 #define TODGPU_CTA_THREADS 256
 #endif
 constexpr int kNT = TODGPU_CTA_THREADS;  // threads per CTA
+// Beams of at least this many pixels (16 per thread) take the shared float64
+// parameter mode in the single-launch kernel (measured: S = 9530 runs 3-6%
+// faster shared; S = 1512 runs 8-11% slower shared, hence the threshold).
+constexpr long long kShareRotMinS = 16LL * kNT;
 
 // CTAs per SM the register budget is sized for: 4 (64 registers) for the
 // nearest mode and packed maps, where the fourth CTA measured 3-5% faster; 3
@@ -1265,7 +1275,9 @@ int dispatch_qu(const KArgs& k, bool has_qu, cudaStream_t s) {
 template <int MODE, typename MapT>
 int dispatch_single_pm(const KArgs& k, bool has_qu, int params_dtype, cudaStream_t s) {
   if (params_dtype == TODGPU_F32) return dispatch_qu<MODE, MapT, kParamsRef32>(k, has_qu, s);
-  if (params_dtype == TODGPU_F64) return dispatch_qu<MODE, MapT, kParamsF64>(k, has_qu, s);
+  if (params_dtype == TODGPU_F64)
+    return k.S >= kShareRotMinS ? dispatch_qu<MODE, MapT, kParamsF64Shared>(k, has_qu, s)
+                                : dispatch_qu<MODE, MapT, kParamsF64>(k, has_qu, s);
   return dispatch_qu<MODE, MapT, kAngles>(k, has_qu, s);
 }
 

@@ -19,11 +19,16 @@ Differences, all additive:
 * a float64 map is kept on the device as float64 records {I, Q, U, 0} (one
   memory sector per pixel; the same TOD bit for bit);
 * ``return_device=True`` returns the (C, B) float64 CUDA accumulator instead
-  of the float32 host dict.
+  of the float32 host dict;
+* a large batch is pipelined: the host prepares the float32 parameters of
+  chunks of samples on a thread pool while the GPU gathers the previous
+  chunks (every parameter is a per-sample function, so the parameters -- and
+  the TOD -- are the same bit for bit as one preparation of the whole batch).
 """
 
 from __future__ import annotations
 
+import os
 import weakref
 
 import numpy as np
@@ -127,6 +132,90 @@ def component_slots(comp_indices):
     return c_q, c_u
 
 
+# Pipelined host preparation of the reference-typed path: samples per chunk,
+# and float32 words per sample in a chunk's upload (axes 3, cos_a, sin_a,
+# ax_pts 3, cos_p, sin_p, bore_phi).
+PIPE_CHUNK = 1 << 19
+_PIPE_WIDTHS = (3, 1, 1, 3, 1, 1, 1)
+_PIPE_WORDS = sum(_PIPE_WIDTHS)
+_prep_pool = None
+
+
+def _pool():
+    global _prep_pool
+    if _prep_pool is None:
+        from concurrent.futures import ThreadPoolExecutor
+
+        _prep_pool = ThreadPoolExecutor(max_workers=max(1, min(16, os.cpu_count() or 1)),
+                                        thread_name_prefix="todgpu-prep")
+    return _prep_pool
+
+
+def _prep_chunk(rot_vecs, phi_b, theta_b, psis_b, s0, s1, with_bore):
+    """Float32 parameters of samples [s0, s1), field after field in one buffer."""
+    params = _rotation_params(rot_vecs[s0:s1], phi_b[s0:s1], theta_b[s0:s1], psis_b[s0:s1])
+    n = s1 - s0
+    out = np.empty(_PIPE_WORDS * n, np.float32)
+    o = 0
+    for p, w in zip(params, _PIPE_WIDTHS):
+        out[o:o + w * n] = np.asarray(p, np.float32).reshape(-1)
+        o += w * n
+    out[o:] = boresight_phi_host(params[3]) if with_bore else np.float32(0.0)
+    return out
+
+
+def _gather_pipelined(interp, nside, rot_vecs, phi_b, theta_b, psis_b, vec, bv, mpd, tod, S, c_q, c_u):
+    """beam_tod_batch's gather in chunks of PIPE_CHUNK samples: parameters
+    prepared on the thread pool, uploaded through two pinned staging slots on
+    a copy stream, each chunk's gather launched as soon as its upload lands."""
+    B = tod.shape[1]
+    dev = tod.device
+    with_bore = c_q >= 0 and c_u >= 0
+    chunks = [(s0, min(B, s0 + PIPE_CHUNK)) for s0 in range(0, B, PIPE_CHUNK)]
+    pool = _pool()
+    futs = [pool.submit(_prep_chunk, rot_vecs, phi_b, theta_b, psis_b, a, b, with_bore) for a, b in chunks]
+    width = _PIPE_WORDS * min(B, PIPE_CHUNK)
+    pin = [torch.empty(width, dtype=torch.float32, pin_memory=True) for _ in range(2)]
+    dbuf = [torch.empty(width, dtype=torch.float32, device=dev) for _ in range(2)]
+    comp = torch.cuda.current_stream(dev)
+    up = torch.cuda.Stream(dev)
+    uploaded = [None, None]  # upload of slot k done: pin[k] free, dbuf[k] ready
+    consumed = [None, None]  # gather of slot k done: dbuf[k] free
+    try:
+        for i, ((s0, s1), fut) in enumerate(zip(chunks, futs)):
+            k = i & 1
+            n = s1 - s0
+            host = fut.result()
+            if uploaded[k] is not None:
+                uploaded[k].synchronize()
+            pin[k][:_PIPE_WORDS * n].numpy()[:] = host
+            with torch.cuda.stream(up):
+                if consumed[k] is not None:
+                    up.wait_event(consumed[k])
+                dbuf[k][:_PIPE_WORDS * n].copy_(pin[k][:_PIPE_WORDS * n], non_blocking=True)
+                uploaded[k] = torch.cuda.Event()
+                uploaded[k].record(up)
+            comp.wait_event(uploaded[k])
+            views, o = [], 0
+            for w in _PIPE_WIDTHS:
+                v = dbuf[k][o:o + w * n]
+                views.append(v.view(n, 3) if w == 3 else v)
+                o += w * n
+            gather_accum(interp, vec, *views[:6], nside, mpd, bv, n, S, tod[:, s0:s1], c_q, c_u,
+                         bore_phi=views[6])
+            consumed[k] = torch.cuda.Event()
+            consumed[k].record(comp)
+    finally:
+        for f in futs:
+            f.cancel()
+        for e in uploaded:
+            if e is not None:
+                e.synchronize()
+    for d in dbuf:
+        d.record_stream(up)
+    return tod
+
+
 def beam_tod_batch(nside, mp, data, rot_vecs, phi_b, theta_b, psis_b, interp_mode="bilinear",
                    *, return_device=False):
     """GPU replacement of ``tod_core.beam_tod_batch`` (tod_core.py:52-167)."""
@@ -142,14 +231,19 @@ def beam_tod_batch(nside, mp, data, rot_vecs, phi_b, theta_b, psis_b, interp_mod
             f"interp_mode {interp_mode!r} not available on main branch; "
             "switch to the 'gaussian' or 'bicubic' branch")
     require_cuda()
-    params = _rotation_params(rot_vecs, phi_b, theta_b, psis_b)
-    bore_phi = boresight_phi_host(params[3]) if (c_q >= 0 and c_u >= 0) else None
     vec = _cache.get(vec_orig, torch.float32)
     bv = _cache.get(beam_vals, torch.float32)
     mpd = device_map(data, mp)
     tod = torch.zeros((C, B), dtype=torch.float64, device=mpd.device)
-    gather_accum(_INTERP[interp_mode], vec, *params, nside, mpd, bv, B, S, tod, c_q, c_u,
-                 bore_phi=bore_phi if bore_phi is not None else np.zeros(B, np.float32))
+    host_inputs = not any(is_tensor(x) for x in (rot_vecs, phi_b, theta_b, psis_b))
+    if host_inputs and B > PIPE_CHUNK and S > 0:
+        _gather_pipelined(_INTERP[interp_mode], nside, np.asarray(rot_vecs), np.asarray(phi_b),
+                          np.asarray(theta_b), np.asarray(psis_b), vec, bv, mpd, tod, S, c_q, c_u)
+    else:
+        params = _rotation_params(rot_vecs, phi_b, theta_b, psis_b)
+        bore_phi = boresight_phi_host(params[3]) if (c_q >= 0 and c_u >= 0) else None
+        gather_accum(_INTERP[interp_mode], vec, *params, nside, mpd, bv, B, S, tod, c_q, c_u,
+                     bore_phi=bore_phi if bore_phi is not None else np.zeros(B, np.float32))
     if return_device:
         return tod
     host = tod.to(torch.float32).cpu().numpy()

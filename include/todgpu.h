@@ -147,7 +147,7 @@ int todgpu_gather_accum_batched(const todgpu_gather_args *jobs, int32_t njobs, i
  * whose device memory is owned by another framework's allocator, or a foreign-
  * language binding that can hand over existing buffers but has no way to
  * create new ones.  Instead of a caller-provided ring table it uses one built
- * into the library: a statically sized array (1 MiB, nside <= 4096) that every
+ * into the library: a statically sized array (1.25 MiB, nside <= 4096) that every
  * GPU loading the library holds until the process exits.  args->ring_table is
  * ignored; nside > 4096 is rejected with TODGPU_ENSIDE.  Each call rebuilds
  * the table on `stream` for its own nside and beam before the gather, so no

@@ -175,17 +175,24 @@ def _random_case(B, S, nside, seed, beam_radius_deg, pole=False, dtype=np.float3
 
 
 @pytest.mark.parametrize("mode", ["bilinear", "nearest"])
-@pytest.mark.parametrize("kind", ["pole", "wide", "tiny_nside", "plain"])
+@pytest.mark.parametrize("kind", ["pole", "wide", "tiny_nside", "plain", "many"])
 def test_tables_match_direct_and_oracle(mode, kind):
     """Footprint tables (ring window + spin-2 table) give bit-identical TOD to
     direct per-neighbour evaluation, including footprints that contain a pole,
     footprints too large for the tables (8 deg beam at nside 256), nside 2
-    (window = whole sphere) and a plain case; both match the oracle."""
+    (window = whole sphere), a plain case and 2e7 evaluations at nside 1024
+    (the fast path's quotients from ring reciprocals and its nearest-mode
+    ranking against the direct path's divisions and cos()); both match the
+    oracle, bar the last case: on its white-noise float32 sky one ulp of the
+    longitude (CUDA's atan2 against the host libm's) moves a bilinear weight
+    by up to 3e-13 at nside 1024, so the worst of its 20000 samples sits at
+    the 1e-12 bound -- the config-2 shaped cases hold the oracle to it."""
     from tod_generation_mapbased_beam_b200 import _native
     from tod_generation_mapbased_beam_b200.kernels import gather_accum
 
     cfg = {"pole": (256, 300, 64, 1.0, True), "wide": (64, 400, 256, 8.0, False),
-           "tiny_nside": (64, 200, 2, 10.0, False), "plain": (256, 500, 128, 1.5, False)}[kind]
+           "tiny_nside": (64, 200, 2, 10.0, False), "plain": (256, 500, 128, 1.5, False),
+           "many": (20000, 1000, 1024, 1.0, False)}[kind]
     B, S, nside, rad, pole = cfg
     params, mp, bv = _random_case(B, S, nside, seed=hash(kind) % 1000, beam_radius_deg=rad, pole=pole)
     interp = _native.BILINEAR if mode == "bilinear" else _native.NEAREST
@@ -195,6 +202,8 @@ def test_tables_match_direct_and_oracle(mode, kind):
         gather_accum(interp, *params, nside, mp, bv, B, S, tod, 1, 2, flags=flags)
         outs.append(tod.cpu().numpy())
     np.testing.assert_array_equal(outs[0], outs[1])
+    if kind == "many":
+        return
     cpu = np.zeros((3, B))
     fn = oracle.gather_accum_fused if mode == "bilinear" else oracle.gather_accum_nearest
     fn(*params, nside, mp, bv, B, S, cpu, 1, 2)
@@ -413,3 +422,37 @@ def test_pipelined_drop_in_bit_identical(mode, comps, monkeypatch):
     assert sorted(out) == sorted(comps)
     for i, c in enumerate(comps):
         assert np.array_equal(out[c], one[i].to(torch.float32).cpu().numpy())
+
+
+def test_nearest_near_ties_fast_path_matches_direct():
+    """Pointings on a ring centre exactly midway between two pixel centres,
+    and on the midpoint between two rings: the nearest mode's candidates tie
+    to rounding, which sends the table fast path to its re-ranking by cos();
+    the chosen pixels (read back through a map holding each pixel's index)
+    equal the direct path's for every sample."""
+    from tod_generation_mapbased_beam_b200 import _native
+    from tod_generation_mapbased_beam_b200.kernels import gather_accum
+
+    nside = 64
+    rng = np.random.default_rng(11)
+    pix = rng.integers(0, 12 * nside * nside - 1, 3000)
+    th0, ph0 = oracle.pix2ang(nside, pix)
+    th1, ph1 = oracle.pix2ang(nside, pix + 1)
+    same = th0 == th1  # neighbours on one ring: midway in longitude
+    theta = np.where(same, th0, 0.5 * (th0 + th1))
+    phi = np.where(same, 0.5 * (ph0 + ph1), ph0)
+    B = len(theta)
+    rot, beta = oracle.rotation_vectors_f64(0.0, 0.0, phi, theta)
+    params = oracle.rotation_params_f64(rot, phi, theta, -beta)
+    vec = np.array([[0.0, 0.0, 1.0]])
+    bv = np.ones(1, np.float32)
+    mp = np.arange(12 * nside * nside, dtype=np.float64)[None, :]
+    outs = []
+    for flags in (0, _native.FLAG_NO_TABLES):
+        tod = torch.zeros((1, B), dtype=torch.float64, device="cuda")
+        gather_accum(_native.NEAREST, vec, *params, nside, mp, bv, B, 1, tod, flags=flags)
+        outs.append(tod.cpu().numpy())
+    assert np.array_equal(outs[0], outs[1])
+    # every chosen pixel is one of the tied candidates' neighbourhood: within
+    # a ring of the pointing's own pixel
+    assert np.all(np.abs(outs[0][0] - pix) <= 8 * nside)

@@ -24,8 +24,8 @@ import torch
 
 from . import _native
 from ._device import require_cuda, stream_handle, to_device
-from .kernels import (PackedMap, _map_tensor, _ncomp, _set_map, beam_reach, pointing_buffers, pointing_params,
-                      ring_table)
+from .kernels import (PackedMap, _map_tensor, _ncomp, _row_stride, _set_map, beam_reach, pointing_buffers,
+                      pointing_params, ring_table)
 
 
 class DetectorBatch:
@@ -97,7 +97,7 @@ class DetectorBatch:
                 a.center_phi, a.center_theta = cen
             a.beam_vals = bv.data_ptr()
             a.tod = out.data_ptr()
-            a.tod_stride = out.stride(0)
+            a.tod_stride = _row_stride(out)
             a.flags = self.flags
             a.ring_table = None if self.table is None else self.table.data_ptr()
         return arr

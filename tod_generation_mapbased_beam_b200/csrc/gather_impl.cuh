@@ -367,8 +367,10 @@ struct __align__(16) RingRec {
   int n;         // pixels in the ring
   int cap;       // spin-2 table slots reserved for this ring
   long long pre; // sum of cap over rings 1 .. ir-1
+  double inv_dphi;  // 1 / dphi, correctly rounded
+  double inv_dta;   // 1 / (ta(ir + 1) - ta), correctly rounded (0 for the last ring)
 };
-static_assert(sizeof(RingRec) == 64, "RingRec must be 64 bytes");
+static_assert(sizeof(RingRec) == 80, "RingRec must be 80 bytes");
 
 // Ring provider backed by the global ring table.
 struct TableRings {
@@ -588,7 +590,7 @@ constexpr int kLayoutIQU = 1;      // C = 3, Q at 1, U at 2
 
 struct RingFast {
   int n, first;
-  double phi0, dphi, z, ta;
+  double phi0, dphi, z, ta, inv_dphi, inv_dta;
 };
 
 __device__ __forceinline__ RingFast ring_fast(const RingRec* rt, int ir) {
@@ -600,6 +602,8 @@ __device__ __forceinline__ RingFast ring_fast(const RingRec* rt, int ir) {
   d.dphi = __ldg(&r->dphi);
   d.z = __ldg(&r->z);
   d.ta = __ldg(&r->ta);
+  d.inv_dphi = __ldg(&r->inv_dphi);
+  d.inv_dta = __ldg(&r->inv_dta);
   return d;
 }
 
@@ -618,6 +622,29 @@ __device__ __forceinline__ int wrap_up(int x, int d, int n) {
   const int v = x + d;
   return v >= n ? v - n : v;
 }
+
+// cos(d) for |d| <= kCosSmallMax by its Taylor series through d^6 (the first
+// term left out, d^8 / 8!, is below 7e-19 there), in Horner form in d^2.
+constexpr double kCosSmallMax = 0.02;
+__device__ __forceinline__ double cos_small(double d) {
+  const double u = d * d;
+  return fma(u, fma(u, fma(u, -1.0 / 720.0, 1.0 / 24.0), -0.5), 1.0);
+}
+
+// x / d correctly rounded, from y = 1 / d correctly rounded: the quotient
+// x y and two residual corrections by Markstein's theorem (P. Markstein, IBM
+// J. Res. Dev. 34(1), 1990: with y within half an ulp of 1/d and q within
+// one ulp of x/d, the residual r = x - q d is exact under fma and
+// fma(r, y, q) is x/d rounded to nearest).  The first correction brings x y
+// (within two ulps) within one ulp, the second rounds correctly.  For finite
+// x and d whose quotient and residuals stay in the normal range -- the ring,
+// weight and longitude quotients here (|x| < 1e6, 1e-5 < |d| < 7).
+__device__ __forceinline__ double div_rn(double x, double d, double y) {
+  const double q0 = x * y;
+  const double q1 = fma(fma(-q0, d, x), y, q0);
+  return fma(fma(-q1, d, x), y, q1);
+}
+constexpr double kInvTwoPi = 1.0 / kTwoPi;
 
 // The bilinear stencil of hp_stencil with 32-bit indices; tw is in [0, n]
 // for finite phi in [0, 2 pi], so int(tw) is a plain truncation.
@@ -659,15 +686,15 @@ __device__ __forceinline__ void stencil_fast(int nside, double z, double phi_w, 
     const RingFast rb = ring_fast(rt, ir_below);
     double dta;
     if (!dtheta_small(z, ra.z, __ldg(&rt[ir_above].sth), dta)) dta = acos(z) - ra.ta;
-    const double wb = dta / (rb.ta - ra.ta);
+    const double wb = div_rn(dta, rb.ta - ra.ta, ra.inv_dta);
     const double wa = 1.0 - wb;
-    double tw = py_fmod_pos((phi_w - ra.phi0) / ra.dphi, (double)ra.n);
+    double tw = py_fmod_pos(div_rn(phi_w - ra.phi0, ra.dphi, ra.inv_dphi), (double)ra.n);
     const int ia = (int)tw;
     const double fa = tw - (double)ia;
     const int ia1 = wrap_up(ia, 1, ra.n);
     visit(0, ra.first + ia, wa * (1.0 - fa), ir_above, ia, ra.n, ra.z, ra.phi0 + (double)ia * ra.dphi);
     visit(1, ra.first + ia1, wa * fa, ir_above, ia1, ra.n, ra.z, ra.phi0 + (double)ia1 * ra.dphi);
-    tw = py_fmod_pos((phi_w - rb.phi0) / rb.dphi, (double)rb.n);
+    tw = py_fmod_pos(div_rn(phi_w - rb.phi0, rb.dphi, rb.inv_dphi), (double)rb.n);
     const int ib = (int)tw;
     const double fb = tw - (double)ib;
     const int ib1 = wrap_up(ib, 1, rb.n);
@@ -835,31 +862,76 @@ __device__ __forceinline__ void eval_fast(const KArgs& a, const Bore& bo, const 
     } else {
       ir_above = 1;
     }
-    int best_pix = 0, best_ring = 0, best_ip = 0, best_n = 1;
-    double best_cos = -2.0, best_zc = 0.0, best_phic = 0.0;
+    // The four candidates: two pixels on each of rings ir_above and
+    // ir_above + 1, ranked by the cosine of their angular distance.  A first
+    // pass evaluates cos(phi_w - phic) by cos_small where the difference is at
+    // most kCosSmallMax (cos() beyond); the two differ by < 2e-15, so a lead of more
+    // than 1e-13 over the runner-up picks the pixel that ranking by cos()
+    // picks.  A closer call is ranked again by cos() itself -- the same
+    // expression, order and strict comparison -- so the pixel is always the
+    // one of ranking by cos() throughout.
+    int best_ring = -1, best_ip = 0;
+    {
+      double lead = -3.0, runner = -3.0;
 #pragma unroll
-    for (int g = 0; g < 2; ++g) {
-      const int ir = ir_above + g;
-      const RingRec* rr = rt + ir;
-      const int n = __ldg(&rr->n);
-      const double phi0 = __ldg(&rr->phi0), dphi = __ldg(&rr->dphi), zc = __ldg(&rr->z), szc = __ldg(&rr->sth);
-      int ipb = (int)(phi_w * (double)n / kTwoPi);
-      if (ipb >= n) ipb -= n;
+      for (int g = 0; g < 2; ++g) {
+        const int ir = ir_above + g;
+        const RingRec* rr = rt + ir;
+        const int n = __ldg(&rr->n);
+        const double phi0 = __ldg(&rr->phi0), dphi = __ldg(&rr->dphi), zc = __ldg(&rr->z), szc = __ldg(&rr->sth);
+        int ipb = (int)div_rn(phi_w * (double)n, kTwoPi, kInvTwoPi);
+        if (ipb >= n) ipb -= n;
 #pragma unroll
-      for (int t = 0; t < 2; ++t) {
-        const int ip = (t == 0) ? ipb : wrap_up(ipb, 1, n);
-        const double phic = phi0 + (double)ip * dphi;
-        const double cosd = sin_th * szc * cos(phi_w - phic) + vz * zc;
-        if (cosd > best_cos) {
-          best_cos = cosd;
-          best_pix = (int)__ldg(&rr->first) + ip;
-          best_ring = ir;
-          best_ip = ip;
-          best_n = n;
-          best_zc = zc;
-          best_phic = phic;
+        for (int t = 0; t < 2; ++t) {
+          const int ip = (t == 0) ? ipb : wrap_up(ipb, 1, n);
+          const double dl = phi_w - (phi0 + (double)ip * dphi);
+          const double cosd = sin_th * szc * (fabs(dl) <= kCosSmallMax ? cos_small(dl) : cos(dl)) + vz * zc;
+          if (cosd > lead) {
+            runner = lead;
+            lead = cosd;
+            best_ring = ir;
+            best_ip = ip;
+          } else if (cosd > runner) {
+            runner = cosd;
+          }
         }
       }
+      if (!(lead - runner > 1e-13)) {
+        double best_cos = -2.0;
+        best_ring = -1;
+#pragma unroll
+        for (int g = 0; g < 2; ++g) {
+          const int ir = ir_above + g;
+          const RingRec* rr = rt + ir;
+          const int n = __ldg(&rr->n);
+          const double phi0 = __ldg(&rr->phi0), dphi = __ldg(&rr->dphi), zc = __ldg(&rr->z), szc = __ldg(&rr->sth);
+          int ipb = (int)(phi_w * (double)n / kTwoPi);
+          if (ipb >= n) ipb -= n;
+#pragma unroll
+          for (int t = 0; t < 2; ++t) {
+            const int ip = (t == 0) ? ipb : wrap_up(ipb, 1, n);
+            const double phic = phi0 + (double)ip * dphi;
+            const double cosd = sin_th * szc * cos(phi_w - phic) + vz * zc;
+            if (cosd > best_cos) {
+              best_cos = cosd;
+              best_ring = ir;
+              best_ip = ip;
+            }
+          }
+        }
+      }
+    }
+    int best_pix = 0, best_n = 1;
+    double best_zc = 0.0, best_phic = 0.0;
+    if (best_ring >= 0) {
+      const RingRec* rr = rt + best_ring;
+      best_n = __ldg(&rr->n);
+      best_pix = (int)__ldg(&rr->first) + best_ip;
+      best_zc = __ldg(&rr->z);
+      best_phic = __ldg(&rr->phi0) + (double)best_ip * __ldg(&rr->dphi);
+    } else {
+      best_ring = 0;
+      best_ip = 0;
     }
     if constexpr (kPacked) {
       const float4 rec = load_rec<MapT>(a, best_pix);

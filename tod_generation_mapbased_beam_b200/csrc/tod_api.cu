@@ -39,6 +39,8 @@ __global__ void ring_table_kernel(long long nside, double reach, RingRec* t, boo
     }
     r.cap = cap;
     r.pre = 0;
+    r.inv_dphi = 1.0 / ri.dphi;
+    r.inv_dta = ir < nrings ? 1.0 / (acos(hp_ring_z(nside, ir + 1)) - r.ta) : 0.0;
     t[ir] = r;
   }
   if (!reach_from_header && blockIdx.x == 0 && threadIdx.x == 0) {
@@ -52,6 +54,8 @@ __global__ void ring_table_kernel(long long nside, double reach, RingRec* t, boo
     h.n = 0;
     h.cap = 0;
     h.pre = 0;
+    h.inv_dphi = 0.0;
+    h.inv_dta = 0.0;
     t[0] = h;
   }
 }
@@ -243,7 +247,7 @@ __global__ void spin2_kernel(const double* zp, const double* sp, const double* p
 // Built-in ring table for callers that cannot allocate device memory.
 // ---------------------------------------------------------------------------
 
-// Largest nside the built-in table holds: 4 * 4096 records of 64 bytes = 1 MiB,
+// Largest nside the built-in table holds: 4 * 4096 records of 80 bytes = 1.25 MiB,
 // resident on every GPU that loads the library until the process exits.
 constexpr long long kStaticMaxNside = 4096;
 static __device__ __align__(256) RingRec g_static_ring_table[4 * kStaticMaxNside];
@@ -266,6 +270,8 @@ __global__ void __launch_bounds__(kNTStatic) static_reach_kernel(const KArgs a, 
     h.n = 0;
     h.cap = 0;
     h.pre = 0;
+    h.inv_dphi = 0.0;
+    h.inv_dta = 0.0;
     t[0] = h;
   }
 }

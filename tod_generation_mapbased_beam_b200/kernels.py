@@ -121,6 +121,13 @@ def ring_table(nside, reach, device=None):
     return t
 
 
+def _row_stride(t):
+    """Row stride of a (rows, n) tensor with unit column stride; a single
+    row's stride is free in torch (a ``[None, :]`` view may carry 0), so it
+    is taken as n."""
+    return t.stride(0) if t.shape[0] > 1 else t.shape[1]
+
+
 def _set_map(a, mp):
     if isinstance(mp, PackedMap):
         a.map_dtype = mp.map_dtype
@@ -129,7 +136,7 @@ def _set_map(a, mp):
     else:
         a.map_dtype = _native.F32 if mp.dtype == torch.float32 else _native.F64
         a.map = mp.data_ptr()
-        a.map_stride = mp.stride(0)
+        a.map_stride = _row_stride(mp)
 
 
 def _ncomp(mp):
@@ -153,7 +160,7 @@ def make_args(interp, nside, B, S, C, c_q, c_u, params, pdt, bore_phi, beam, mp,
     a.bore_phi = ptr(bore_phi)
     a.beam_vals = ptr(beam)
     a.tod = ptr(tod)
-    a.tod_stride = tod.stride(0)
+    a.tod_stride = _row_stride(tod)
     a.err_count = ptr(err)
     a.flags = int(flags)
     a.ring_table = ptr(table)
@@ -197,7 +204,7 @@ def pack_map(mp_stacked, kind="f32"):
     dt = {"f32": torch.float32, "bf16": torch.bfloat16, "f64": torch.float64}[kind]
     out = torch.empty((N, 4), dtype=dt, device=mp.device)
     _native.check(_native.lib().todgpu_pack_map(
-        mp.data_ptr(), _native.F32 if mp.dtype == torch.float32 else _native.F64, C, N, mp.stride(0),
+        mp.data_ptr(), _native.F32 if mp.dtype == torch.float32 else _native.F64, C, N, _row_stride(mp),
         {"f32": _native.PACKED_F32, "bf16": _native.PACKED_BF16, "f64": _native.PACKED_F64}[kind], out.data_ptr(),
         stream_handle()))
     return PackedMap(out, C, kind)
@@ -400,7 +407,7 @@ def gather_accum_angles(interp, vec_orig, theta, phi, psi, center_phi, center_th
         a.center_theta = float(center_theta)
     a.beam_vals = beam.data_ptr()
     a.tod = tod.data_ptr()
-    a.tod_stride = tod.stride(0)
+    a.tod_stride = _row_stride(tod)
     a.err_count = ptr(err_count)
     a.flags = int(flags)
     lib = _native.lib()

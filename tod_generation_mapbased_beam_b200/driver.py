@@ -37,7 +37,60 @@ from .tod_core import _cache, _INTERP, beam_tod_batch, component_slots, device_m
 from .tod_rotations import precompute_rotation_vector_batch
 
 __all__ = ["load_scan_information", "open_scan_day", "DayRunner", "tod_exact_gen_batched",
-           "process_day"]
+           "process_day", "prepare_beam_data", "load_sky"]
+
+
+def load_sky(path_to_map):
+    """The sky as the reference's main loads it (gridint.py:406-408): fields
+    0, 1, 2 of a HEALPix FITS map, RING order, each cast to float32."""
+    from .map_io import read_map
+
+    return [m.astype(np.float32) for m in read_map(path_to_map, field=(0, 1, 2))]
+
+
+def prepare_beam_data(beam_filenames, folder_beam=None, thresholds=None, config=None):
+    """Drop-in for ``prepare_beam_data`` (gridint.py:92-159): one entry per
+    distinct beam file, keyed by file name, with ``ra, dec`` (offset grids as
+    ``load_beam`` binds them), ``beam_vals`` (float32, normalised by their sum
+    unless it is 0), ``sel`` (``10 log10(|b| + 1e-30) > dB cut`` for the
+    file's power threshold), ``comp_indices`` (the Stokes components sharing
+    the file, in order), ``n_sel`` and ``vec_orig`` (float32 (S, 3): theta =
+    pi/2 - dec, longitude ra).
+
+    ``folder_beam`` and ``thresholds`` ({file name: power fraction}) default to
+    a :class:`tod_config.TodConfig`'s FOLDER_BEAM and its I, Q, U thresholds
+    (a file named for several components takes the last one, as the
+    reference's dictionary does)."""
+    from .map_io import load_beam
+    from .workloads import compute_db_threshold_from_power
+
+    if config is not None:
+        folder_beam = config.FOLDER_BEAM if folder_beam is None else folder_beam
+        if thresholds is None:
+            thresholds = {config.beam_file_I: config.power_threshold_I,
+                          config.beam_file_Q: config.power_threshold_Q,
+                          config.beam_file_U: config.power_threshold_U}
+    if folder_beam is None or thresholds is None:
+        raise ValueError("give folder_beam and thresholds, or a config")
+    groups = {}
+    for i, bf in enumerate(beam_filenames):
+        groups.setdefault(bf, []).append(i)
+    beam_data = {}
+    for bf, comp_indices in groups.items():
+        ra, dec, pixel_map = load_beam(folder_beam, bf)
+        db_cut = compute_db_threshold_from_power(pixel_map, thresholds[bf])
+        with np.errstate(divide="ignore", invalid="ignore"):
+            sel = 10 * np.log10(np.abs(pixel_map) + 1e-30) > db_cut
+        beam_vals = pixel_map[sel].astype(np.float32)
+        norm = beam_vals.sum()
+        if norm != 0:
+            beam_vals /= norm
+        theta_orig = np.pi / 2 - dec
+        vec_orig = np.stack([np.sin(theta_orig) * np.cos(ra), np.sin(theta_orig) * np.sin(ra),
+                             np.cos(theta_orig)], axis=-1)[sel].astype(np.float32)
+        beam_data[bf] = {"ra": ra, "dec": dec, "beam_vals": beam_vals, "sel": sel,
+                         "comp_indices": comp_indices, "n_sel": int(sel.sum()), "vec_orig": vec_orig}
+    return beam_data
 
 
 def load_scan_information(folder):

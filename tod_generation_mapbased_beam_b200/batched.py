@@ -46,7 +46,7 @@ class DetectorBatch:
         self.c_u = comps.index(2) if 2 in comps else -1
         dev = torch.device("cuda", torch.cuda.current_device())
         self.vec, self.beam, self.angles, self.out, self.centers = [], [], [], [], []
-        reach = 0.0
+        self.tables = []
         for d in detectors:
             vec = to_device(d["vec_orig"], np.float64).reshape(-1, 3)
             self.vec.append(vec)
@@ -55,10 +55,13 @@ class DetectorBatch:
             self.angles.append(ang)
             self.out.append(torch.zeros((self.C, ang[0].shape[0]), dtype=torch.float64, device=dev))
             self.centers.append(tuple(d.get("center", (0.0, 0.0))))
-            if vec.shape[0]:
-                reach = max(reach, beam_reach(vec, self.nside))
+            # each detector's own ring table, sized for its own beam: the per-sample
+            # spin-2 tables fill every window ring's reserved slots, so a table
+            # sized for the widest beam of the batch costs the narrower ones work
+            # (tables are cached per reach and shared between equal beams)
+            reach = beam_reach(vec, self.nside) if (tables and vec.shape[0]) else 0.0
+            self.tables.append(ring_table(self.nside, reach, dev) if reach > 0 else None)
         self.rot = [pointing_buffers(a[0].shape[0], dev) for a in self.angles] if precompute else None
-        self.table = ring_table(self.nside, reach, dev) if (tables and reach > 0) else None
         self.flags = 0 if tables else _native.FLAG_NO_TABLES
         self._args = self._make_args()
         self.tile = int(tile) if tile else None
@@ -99,7 +102,7 @@ class DetectorBatch:
             a.tod = out.data_ptr()
             a.tod_stride = _row_stride(out)
             a.flags = self.flags
-            a.ring_table = None if self.table is None else self.table.data_ptr()
+            a.ring_table = None if self.tables[j] is None else self.tables[j].data_ptr()
         return arr
 
     def truncated(self, fraction):

@@ -987,6 +987,83 @@ __device__ __forceinline__ void flush_sample(const KArgs& a, const double* s_red
   }
 }
 
+// Footprint window of one sample, by the kSetupThreads setup threads (warps
+// 0 and 1) together: the window rings about the footprint centre u, each
+// ring's slots and their offsets in the spin-2 table, into w.  Out of line so
+// that its registers do not weigh on the evaluation loop around it.
+constexpr int kSetupThreads = 64;
+static __device__ __noinline__ void footprint_window(const KArgs& a, const RingRec* rt, Spin2Tab& w, double ux,
+                                                     double uy, double uz, double reach) {
+  const int lane = threadIdx.x & 31;
+  const double theta_u = acos(clamp1(uz));
+  double phi_u = atan2(uy, ux);
+  if (phi_u < 0.0) phi_u += kTwoPi;
+  const double th_lo = theta_u - reach, th_hi = theta_u + reach;
+  long long ir_lo = th_lo <= 0.0 ? 1 : hp_ring_above(a.nside, cos(th_lo));
+  long long ir_hi = th_hi >= kPi ? 4 * a.nside - 1 : hp_ring_above(a.nside, cos(th_hi)) + 1;
+  ir_lo = max(ir_lo, 1LL);
+  ir_hi = min(ir_hi, 4 * a.nside - 1);
+  // a non-finite footprint centre gives an empty or invalid window: no table
+  const long long nr = ir_hi - ir_lo + 1;
+  bool fits = nr > 0 && nr <= kRingCap && ir_lo >= 1 && ir_hi <= 4 * a.nside - 1;
+  // Slots per window ring: the ring's stretch of the footprint disc (radius
+  // reach about (theta_u, phi_u)), at most what the ring table reserves
+  // for any footprint of that reach.  Away from the poles the disc's
+  // half-width in longitude on a ring at colatitude theta_r is
+  // sqrt(reach^2 - (theta_r - theta_u)^2) / sin theta_r to within a
+  // percent for reach < 0.05; 5% margin and one pixel either side keep
+  // every stencil pixel in.  (A pixel outside its ring's slots is still
+  // evaluated, directly; only the cost changes.)
+  const bool disc = reach < 0.05 && theta_u - reach > 0.1 && theta_u + reach < kPi - 0.1;
+  if (fits) {
+    for (int t = threadIdx.x; t < nr; t += kSetupThreads) {
+      const RingRec* r = rt + ir_lo + t;
+      const int n = __ldg(&r->n);
+      int cnt = __ldg(&r->cap);
+      if (disc) {
+        const double dth = __ldg(&r->ta) - theta_u;
+        const double h2 = reach * reach - dth * dth;
+        const int k = h2 > 0.0 ? (int)ceil(1.05 * sqrt(h2) / __ldg(&r->sth) * __ldg(&r->inv_dphi)) : 0;
+        cnt = min(cnt, 2 * k + 3);
+      }
+      int iplo = 0;
+      if (cnt < n) {
+        const double c = floor((phi_u - __ldg(&r->phi0)) / __ldg(&r->dphi));
+        iplo = (int)py_imod((long long)c - (cnt - 1) / 2, n);
+      }
+      w.iplo[t] = iplo;
+      w.cap[t] = cnt;
+    }
+  }
+  // slot offsets: exclusive prefix sum of the counts, by warp 0 once both
+  // setup warps have written theirs
+  asm volatile("bar.sync 1, %0;" ::"n"(kSetupThreads) : "memory");
+  if (threadIdx.x < 32) {
+    int carry = 0;
+    if (fits) {
+      for (int b0 = 0; b0 < (int)nr; b0 += 32) {
+        const int t = b0 + lane;
+        const int own = t < nr ? w.cap[t] : 0;
+        int v = own;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+          const int y = __shfl_up_sync(0xffffffffu, v, o);
+          if (lane >= o) v += y;
+        }
+        if (t < nr) w.off[t] = carry + v - own;
+        carry += __shfl_sync(0xffffffffu, v, 31);
+      }
+    }
+    fits = fits && carry <= a.tab_cap;
+    if (threadIdx.x == 0) {
+      w.ir_lo = ir_lo;
+      w.ir_lo32 = (int)ir_lo;
+      w.nr = fits ? (int)nr : 0;
+      w.total = fits ? carry : 0;
+    }
+  }
+}
+
 // Samples of tiles t = t_begin, t_begin + t_step, ... < t_end of one job (one
 // beam entry over one batch of samples; tile t holds samples [t tile,
 // min(B, (t + 1) tile))), by the whole CTA.  With a ring table:
@@ -1002,7 +1079,6 @@ __device__ void run_samples(const KArgs& a, long long t_begin, long long t_end, 
   using Acc = typename std::conditional<MapTraits<MapT>::packed, AccKahan, Acc64>::type;
   TabT* tab = reinterpret_cast<TabT*>(smem_raw + ((sizeof(Spin2Tab) + 15) & ~size_t(15)));
 
-  constexpr int kSetupThreads = 64;  // threads that derive a sample's footprint window
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const RingRec* rt = static_cast<const RingRec*>(a.ring_table);
   const bool fast = rt != nullptr && a.nside <= 8192;
@@ -1067,43 +1143,7 @@ __device__ void run_samples(const KArgs& a, long long t_begin, long long t_end, 
         // footprint window of this sample (same values in every setup thread)
         double ux, uy, uz;
         rot_f64(rot, cx, cy, cz, ux, uy, uz);
-        const double theta_u = acos(clamp1(uz));
-        double phi_u = atan2(uy, ux);
-        if (phi_u < 0.0) phi_u += kTwoPi;
-        const double th_lo = theta_u - reach, th_hi = theta_u + reach;
-        long long ir_lo = th_lo <= 0.0 ? 1 : hp_ring_above(a.nside, cos(th_lo));
-        long long ir_hi = th_hi >= kPi ? 4 * a.nside - 1 : hp_ring_above(a.nside, cos(th_hi)) + 1;
-        ir_lo = max(ir_lo, 1LL);
-        ir_hi = min(ir_hi, 4 * a.nside - 1);
-        // a non-finite footprint centre gives an empty or invalid window: no table
-        const long long nr = ir_hi - ir_lo + 1;
-        bool fits = nr > 0 && nr <= kRingCap && ir_lo >= 1 && ir_hi <= 4 * a.nside - 1;
-        long long base = 0, total = 0;
-        if (fits) {
-          base = __ldg(&rt[ir_lo].pre);
-          total = __ldg(&rt[ir_hi].pre) + __ldg(&rt[ir_hi].cap) - base;
-          fits = total <= a.tab_cap;
-        }
-        if (fits) {
-          for (int t = threadIdx.x; t < nr; t += kSetupThreads) {
-            const RingRec* r = rt + ir_lo + t;
-            const int n = __ldg(&r->n), cap = __ldg(&r->cap);
-            int iplo = 0;
-            if (cap < n) {
-              const double c = floor((phi_u - __ldg(&r->phi0)) / __ldg(&r->dphi));
-              iplo = (int)py_imod((long long)c - (cap - 1) / 2, n);
-            }
-            w.off[t] = (int)(__ldg(&r->pre) - base);
-            w.iplo[t] = iplo;
-            w.cap[t] = cap;
-          }
-        }
-        if (threadIdx.x == 0) {
-          w.ir_lo = ir_lo;
-          w.ir_lo32 = (int)ir_lo;
-          w.nr = fits ? (int)nr : 0;
-          w.total = fits ? (int)total : 0;
-        }
+        footprint_window(a, rt, w, ux, uy, uz, reach);
       }
       __syncthreads();
       const int ntab = w.total, nwin = w.nr;

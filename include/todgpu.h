@@ -110,7 +110,12 @@ typedef struct todgpu_gather_args {
   int64_t tod_stride;
   unsigned long long *err_count; /* optional */
   int32_t flags;         /* TODGPU_FLAG_* */
-  int32_t reserved;
+  int32_t tab_slots;     /* spin-2 table slots per sample in shared memory (with a
+                            ring table and Q, U): 0 keeps the default of 2048 float64
+                            / 4096 float32 pairs; a footprint's worth (about
+                            3.15 reach^2 nside^2 + 15 reach nside + 15, plus margin)
+                            leaves the rest of the SM's memory to L1.  Capped to what
+                            the kernel's CTAs per SM can share.  Must be >= 0. */
   const void *ring_table;/* optional: table built by todgpu_ring_table_build for this
                             nside; NULL evaluates ring data and spin-2 angles directly */
   const void *theta;     /* (B,) boresight colatitude (TODGPU_ANGLES) */

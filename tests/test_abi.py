@@ -65,6 +65,7 @@ def _args(**kw):
     (dict(params_dtype=9), _native.EDTYPE),
     (dict(map_stride=10), _native.ESHAPE),
     (dict(B=-1), _native.ESHAPE),
+    (dict(tab_slots=-1), _native.EINVAL),
     (dict(B=4, S=4, tod_stride=4), _native.EINVAL),  # NULL pointers with work to do
 ])
 def test_argument_validation(kw, code):
@@ -92,3 +93,14 @@ def test_boresight_phi_host_matches_libm_atan2f():
 
     got = boresight_phi_host(pts)
     np.testing.assert_array_equal(got, oracle.atan2f(pts[:, 1], pts[:, 0]))
+
+
+def test_table_slots_request():
+    """Spin-2 table slots asked for per call: a footprint's worth for small
+    reaches (grows with reach and nside), the default beyond 0.05 rad."""
+    from tod_generation_mapbased_beam_b200 import kernels as K
+
+    assert K.table_slots(1024, 0.0143) < K.table_slots(2048, 0.0143) < K.table_slots(2048, 0.02)
+    assert 900 < K.table_slots(1024, 0.0143) < 1200  # config 2: ~1.05 x 3 r^2 n^2 + 5 per ring, +10%
+    assert K.table_slots(256, 0.05) == 0 and K.table_slots(256, 0.2) == 0
+    assert K.table_slots_for(None, 1024) == 0

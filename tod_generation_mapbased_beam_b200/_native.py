@@ -56,7 +56,7 @@ class GatherArgs(ctypes.Structure):
         ("tod_stride", _i64),
         ("err_count", _p),
         ("flags", _i32),
-        ("reserved", _i32),
+        ("tab_slots", _i32),
         ("ring_table", _p),
         ("theta", _p),
         ("phi", _p),

@@ -25,7 +25,7 @@ import torch
 from . import _native
 from ._device import require_cuda, stream_handle, to_device
 from .kernels import (PackedMap, _map_tensor, _ncomp, _row_stride, _set_map, beam_reach, pointing_buffers,
-                      pointing_params, ring_table)
+                      pointing_params, ring_table, table_slots_for)
 
 
 class DetectorBatch:
@@ -103,6 +103,7 @@ class DetectorBatch:
             a.tod_stride = _row_stride(out)
             a.flags = self.flags
             a.ring_table = None if self.tables[j] is None else self.tables[j].data_ptr()
+            a.tab_slots = table_slots_for(self.tables[j], self.nside)
         return arr
 
     def truncated(self, fraction):

@@ -67,6 +67,7 @@ struct KArgs {
   long long nside, npix, B, S;
   int C, c_q, c_u;
   int tab_cap;               // spin-2 table slots in shared memory
+  int tab_req;               // slots the caller asks for (0: default)
   const void* ring_table;    // RingRec[4 nside] or nullptr
   const void* vec;
   const void* axes;
@@ -1274,8 +1275,16 @@ inline int sm_count() {
 
 struct LaunchInfo {
   int blocks_per_sm = 0;
+  size_t smem = 0;  // dynamic shared memory blocks_per_sm was computed for
   bool configured = false;
 };
+
+// Shared memory per SM on B200 and what the driver keeps per CTA; the
+// kernels' static shared memory (partial sums, rotation slots) stays well
+// under the 2 KiB margin below.
+constexpr size_t kSmemPerSM = 228 * 1024;
+constexpr size_t kSmemPerCTAReserved = 1024;
+constexpr size_t kStaticSmemMargin = 2048;
 
 constexpr size_t kTabHeaderBytes = (sizeof(Spin2Tab) + 15) & ~size_t(15);
 #ifndef TODGPU_CTA_THREADS
@@ -1300,31 +1309,57 @@ constexpr int min_blocks() {
 #endif
 }
 
+// Spin-2 table slots of a launch: the caller's request, else 32 KiB (2048
+// float64 or 4096 float32 pairs); never more than each of MINB CTAs can hold
+// in an SM's shared memory.
+template <typename TabT, int MINB>
+constexpr int max_table_slots() {
+  return (int)((kSmemPerSM / MINB - kSmemPerCTAReserved - kStaticSmemMargin - kTabHeaderBytes) / sizeof(TabT));
+}
+template <typename TabT, int MINB>
+int table_slots(int requested) {
+  constexpr int kCap = (int)(kTabCapDefault * sizeof(double2) / sizeof(TabT));
+  return requested > 0 ? std::min(requested, max_table_slots<TabT, MINB>()) : kCap;
+}
+
+// Once per kernel: allow the largest table; per launch: CTAs per SM for the
+// launch's shared memory (recomputed when it changes).
+template <typename TabT, int MINB, typename Kern>
+int configure_launch(Kern kern, LaunchInfo& info, std::mutex& mu, size_t smem, int& blocks_per_sm) {
+  constexpr int kCap = (int)(kTabCapDefault * sizeof(double2) / sizeof(TabT));
+  constexpr size_t smem_limit =
+      kTabHeaderBytes + sizeof(TabT) * (size_t)std::max(kCap, max_table_slots<TabT, MINB>());
+  std::lock_guard<std::mutex> lock(mu);
+  if (!info.configured) {
+    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_limit);
+    if (e != cudaSuccess) return cuda_fail(e, "cudaFuncSetAttribute");
+    info.configured = true;
+    info.blocks_per_sm = 0;
+  }
+  if (info.blocks_per_sm == 0 || info.smem != smem) {
+    int nb = 0;
+    cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, kern, kNT, smem);
+    if (e != cudaSuccess) return cuda_fail(e, "cudaOccupancyMaxActiveBlocksPerMultiprocessor");
+    info.blocks_per_sm = std::max(nb, 1);
+    info.smem = smem;
+  }
+  blocks_per_sm = info.blocks_per_sm;
+  return TODGPU_OK;
+}
+
 template <int MODE, bool HAS_QU, typename MapT, int PM, int LAYOUT>
 int launch_gather(KArgs k, cudaStream_t stream) {
   auto kern = gather_accum_kernel<MODE, HAS_QU, MapT, PM, LAYOUT, kNT, min_blocks<MODE, MapT>()>;
   static LaunchInfo info;
   static std::mutex mu;
   using TabT = typename MapTraits<MapT>::Tab;
-  // 32 KiB of spin-2 table: 2048 float64 pairs or 4096 float32 pairs
-  constexpr int kCap = (int)(kTabCapDefault * sizeof(double2) / sizeof(TabT));
-  const int tab_cap = (HAS_QU && k.ring_table != nullptr) ? kCap : 0;
+  const int tab_cap = (HAS_QU && k.ring_table != nullptr) ? table_slots<TabT, min_blocks<MODE, MapT>()>(k.tab_req) : 0;
   const size_t smem = kTabHeaderBytes + sizeof(TabT) * (size_t)tab_cap;
-  const size_t smem_max = kTabHeaderBytes + sizeof(TabT) * (size_t)kCap;
-  {
-    std::lock_guard<std::mutex> lock(mu);
-    if (!info.configured) {
-      cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_max);
-      if (e != cudaSuccess) return cuda_fail(e, "cudaFuncSetAttribute");
-      int nb = 0;
-      e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, kern, kNT, smem_max);
-      if (e != cudaSuccess) return cuda_fail(e, "cudaOccupancyMaxActiveBlocksPerMultiprocessor");
-      info.blocks_per_sm = std::max(nb, 1);
-      info.configured = true;
-    }
-  }
+  int blocks_per_sm = 0;
+  const int rc = configure_launch<TabT, min_blocks<MODE, MapT>()>(kern, info, mu, smem, blocks_per_sm);
+  if (rc != TODGPU_OK) return rc;
   k.tab_cap = tab_cap;
-  const long long max_blocks = (long long)sm_count() * info.blocks_per_sm;
+  const long long max_blocks = (long long)sm_count() * blocks_per_sm;
   const int grid = (int)std::max(1LL, std::min(k.B, max_blocks));
   kern<<<grid, kNT, smem, stream>>>(k);
   cudaError_t e = cudaGetLastError();
@@ -1341,26 +1376,23 @@ int launch_batched(BatchParams& bp, bool any_table, cudaStream_t stream) {
   static LaunchInfo info;
   static std::mutex mu;
   using TabT = typename MapTraits<MapT>::Tab;
-  constexpr int kCap = (int)(kTabCapDefault * sizeof(double2) / sizeof(TabT));
-  const int tab_cap = (HAS_QU && any_table) ? kCap : 0;
-  const size_t smem = kTabHeaderBytes + sizeof(TabT) * (size_t)tab_cap;
-  const size_t smem_max = kTabHeaderBytes + sizeof(TabT) * (size_t)kCap;
-  {
-    std::lock_guard<std::mutex> lock(mu);
-    if (!info.configured) {
-      cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_max);
-      if (e != cudaSuccess) return cuda_fail(e, "cudaFuncSetAttribute");
-      int nb = 0;
-      e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, kern, kNT, smem_max);
-      if (e != cudaSuccess) return cuda_fail(e, "cudaOccupancyMaxActiveBlocksPerMultiprocessor");
-      info.blocks_per_sm = std::max(nb, 1);
-      info.configured = true;
-    }
+  // one table size for the launch: the largest any job asks for (a job asking
+  // for the default makes it the default)
+  int req = 0;
+  bool any_default = false;
+  for (int j = 0; j < bp.njobs; ++j) {
+    req = std::max(req, bp.job[j].tab_req);
+    any_default = any_default || bp.job[j].tab_req == 0;
   }
+  const int tab_cap = (HAS_QU && any_table) ? table_slots<TabT, min_blocks<MODE, MapT>()>(any_default ? 0 : req) : 0;
+  const size_t smem = kTabHeaderBytes + sizeof(TabT) * (size_t)tab_cap;
+  int blocks_per_sm = 0;
+  const int rc = configure_launch<TabT, min_blocks<MODE, MapT>()>(kern, info, mu, smem, blocks_per_sm);
+  if (rc != TODGPU_OK) return rc;
   for (int j = 0; j < bp.njobs; ++j) bp.job[j].tab_cap = tab_cap;
   const long long T = bp.tiles_before[bp.njobs];
   if (T == 0) return TODGPU_OK;
-  const long long max_blocks = (long long)sm_count() * info.blocks_per_sm;
+  const long long max_blocks = (long long)sm_count() * blocks_per_sm;
   const int grid = (int)std::max(1LL, std::min(T, max_blocks));
   kern<<<grid, kNT, smem, stream>>>(bp);
   cudaError_t e = cudaGetLastError();

@@ -360,6 +360,7 @@ static int check_common(const todgpu_gather_args* a, bool need_map) {
   if (a->nside < 1 || a->nside > kMaxNside)
     return fail(TODGPU_ENSIDE, "nside " + std::to_string(a->nside) + " outside [1, 16384]");
   if (a->B < 0 || a->S < 0) return fail(TODGPU_ESHAPE, "negative B or S");
+  if (a->tab_slots < 0) return fail(TODGPU_EINVAL, "tab_slots must be >= 0");
   if (a->params_dtype != TODGPU_F32 && a->params_dtype != TODGPU_F64 && a->params_dtype != TODGPU_ANGLES)
     return fail(TODGPU_EDTYPE, "params_dtype must be TODGPU_F32, TODGPU_F64 or TODGPU_ANGLES");
   if (a->B > 0 && a->S > 0) {
@@ -434,6 +435,7 @@ static KArgs make_kargs(const todgpu_gather_args* a) {
   k.ring_table = (a->flags & TODGPU_FLAG_NO_TABLES) ? nullptr : a->ring_table;
   if (k.ring_table != nullptr && (((uintptr_t)k.ring_table & 15) != 0)) k.ring_table = nullptr;
   k.tab_cap = 0;
+  k.tab_req = a->tab_slots;
   return k;
 }
 

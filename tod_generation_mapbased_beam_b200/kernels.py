@@ -21,6 +21,7 @@ parameters give an all-float64 computation.
 from __future__ import annotations
 
 import ctypes
+import math
 import weakref
 
 import numpy as np
@@ -103,6 +104,34 @@ def _beam_reach(vec_orig, nside):
     return r + 3.0 / float(nside) + 2e-5
 
 
+_TABLE_REACH = {}  # data_ptr of a cached ring table -> the reach it was built for
+
+
+def table_slots(nside, reach):
+    """Spin-2 table slots a sample needs for a footprint of radius ``reach``
+    [rad] away from the poles: per window ring the disc's stretch with the
+    kernel's 5% margin and three pixels -- about 1.05 x 3 reach^2 nside^2 for
+    the disc plus 5 per ring over 3 reach nside + 3 rings -- with 10% more
+    and 32 to spare.  Shared memory beyond it is left to L1.  For a reach of
+    0.05 rad or more the kernel reserves whole ring stretches instead of the
+    disc, and the library's default (0) is asked for."""
+    r = float(reach)
+    n = float(nside)
+    if not r < 0.05:
+        return 0
+    need = 1.05 * 3.0 * r * r * n * n + 5.0 * (3.0 * r * n + 3.0)
+    return int(min(1 << 20, math.ceil(1.1 * need) + 32))
+
+
+def table_slots_for(table, nside):
+    """``table_slots`` for a table made by :func:`ring_table` (0, the
+    library's default, for any other table or none)."""
+    if table is None:
+        return 0
+    reach = _TABLE_REACH.get(table.data_ptr()) if is_tensor(table) else None
+    return 0 if reach is None else table_slots(nside, reach)
+
+
 def ring_table(nside, reach, device=None):
     """Device ring table for ``nside`` covering footprints up to ``reach``
     (built once and cached per device, nside and rounded reach)."""
@@ -118,6 +147,7 @@ def ring_table(nside, reach, device=None):
         _native.check(_native.lib().todgpu_ring_table_build(int(nside), float(reach_q), t.data_ptr(),
                                                             nbytes, stream_handle()))
         _RING_TABLES[key] = t
+        _TABLE_REACH[t.data_ptr()] = float(reach_q)
     return t
 
 
@@ -164,6 +194,7 @@ def make_args(interp, nside, B, S, C, c_q, c_u, params, pdt, bore_phi, beam, mp,
     a.err_count = ptr(err)
     a.flags = int(flags)
     a.ring_table = ptr(table)
+    a.tab_slots = table_slots_for(table, nside)
     return a
 
 
@@ -415,6 +446,8 @@ def gather_accum_angles(interp, vec_orig, theta, phi, psi, center_phi, center_th
         _native.check(lib.todgpu_gather_accum_static(ctypes.byref(a), stream_handle()))
         return tod
     if not flags & _native.FLAG_NO_TABLES and B > 0 and S > 0:
-        a.ring_table = ring_table(nside, beam_reach(vec, nside), vec.device).data_ptr()
+        table = ring_table(nside, beam_reach(vec, nside), vec.device)
+        a.ring_table = table.data_ptr()
+        a.tab_slots = table_slots_for(table, nside)
     _native.check(lib.todgpu_gather_accum(ctypes.byref(a), stream_handle()))
     return tod

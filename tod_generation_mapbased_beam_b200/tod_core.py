@@ -171,7 +171,14 @@ def _gather_pipelined(interp, nside, rot_vecs, phi_b, theta_b, psis_b, vec, bv, 
     B = tod.shape[1]
     dev = tod.device
     with_bore = c_q >= 0 and c_u >= 0
-    chunks = [(s0, min(B, s0 + PIPE_CHUNK)) for s0 in range(0, B, PIPE_CHUNK)]
+    # the first chunks ramp up (1/8, 1/4, 1/2 of a chunk) so that the GPU starts
+    # after a short preparation instead of a full chunk's
+    chunks, s0 = [], 0
+    for size in (PIPE_CHUNK >> 3, PIPE_CHUNK >> 2, PIPE_CHUNK >> 1):
+        if s0 < B and size > 0:
+            chunks.append((s0, min(B, s0 + size)))
+            s0 = chunks[-1][1]
+    chunks += [(a, min(B, a + PIPE_CHUNK)) for a in range(s0, B, PIPE_CHUNK)]
     pool = _pool()
     futs = [pool.submit(_prep_chunk, rot_vecs, phi_b, theta_b, psis_b, a, b, with_bore) for a, b in chunks]
     width = _PIPE_WORDS * min(B, PIPE_CHUNK)

@@ -498,6 +498,13 @@ def run_ours(args, dist):
             entry = {"value": B * dist.world / (mms / 1e3), "ms_per_step": mms,
                      "map": {"planar_f64": "planar float64 (C, N), the reference's mp_stacked",
                              "f32": "packed f32 records (16 B/pixel)", "bf16": "packed bf16 records (8 B/pixel)"}[kind]}
+            # the gather view for this map layout: S x K stencil pixels of R bytes
+            # (planar float64: three 8-byte reads per pixel) against the L2 bandwidth
+            rec = {"planar_f64": 24, "f32": 16, "bf16": 8}[kind]
+            gb = float(B) * S * (4 if args.mode == "bilinear" else 1) * rec / (mms / 1e3) / 1e9
+            entry["gather"] = {"bytes_per_sample": S * (4 if args.mode == "bilinear" else 1) * rec,
+                               "achieved": round(gb, 1), "peak": round(l2_peak, 1), "unit": "GB/s",
+                               "frac": round(gb / l2_peak, 4)}
             if kind == "planar_f64":
                 entry["bit_identical_to_value"] = bool(torch.equal(tod, tod_rec))
             elif dist.rank == 0 and not args.no_cpu_baseline:
@@ -582,6 +589,7 @@ def run_precision(args, dist, sky):
 
     dev = torch.device("cuda", dist.local)
     stream = torch.cuda.current_stream(dev)
+    l2_peak = l2_peak_gbs()
     beam = W.pole_gaussian_beam(30.0, 4096, 0.999, search_fwhm=2.0)
     B = args.samples
     th, ph, ps = W.spin_scan(B, 100.0, phi0=0.7 * dist.rank)
@@ -602,10 +610,15 @@ def run_precision(args, dist, sky):
         launch()
         ms = dist.max(_evt_ms(launch, stream))
         subs[kind] = tod[:, idx].cpu().numpy()
+        rec = {"f64": 32, "f32": 16, "bf16": 8}[kind]
+        kk = 4 if args.mode == "bilinear" else 1
+        gb = float(B) * beam.S * kk * rec / (ms / 1e3) / 1e9
         out[kind] = {"value": B * dist.world / (ms / 1e3), "ms_per_step": ms,
                      "map": {"f64": "packed f64 records (32 B/pixel; TOD bit-identical to the planar "
                                     "float64 map)", "f32": "packed f32 records (16 B/pixel)",
-                             "bf16": "packed bf16 records (8 B/pixel)"}[kind]}
+                             "bf16": "packed bf16 records (8 B/pixel)"}[kind],
+                     "gather": {"bytes_per_sample": beam.S * kk * rec, "achieved": round(gb, 1),
+                                "peak": round(l2_peak, 1), "unit": "GB/s", "frac": round(gb / l2_peak, 4)}}
         del tod, mp
     for kind in ("f32", "bf16"):
         out[kind].update(_err_uk(subs[kind], subs["f64"]))

@@ -456,3 +456,39 @@ def test_nearest_near_ties_fast_path_matches_direct():
     # every chosen pixel is one of the tied candidates' neighbourhood: within
     # a ring of the pointing's own pixel
     assert np.all(np.abs(outs[0][0] - pix) <= 8 * nside)
+
+
+@pytest.mark.parametrize("mode", ["bilinear", "nearest"])
+def test_table_slots_change_speed_only(mode):
+    """tab_slots sizes each sample's spin-2 table: far too few slots (the
+    samples do not fit and are evaluated directly), the default, the
+    footprint estimate and more than shared memory holds (capped) all give
+    the same TOD bit for bit, as does a call without the ring table."""
+    import ctypes
+
+    from tod_generation_mapbased_beam_b200 import _native
+    from tod_generation_mapbased_beam_b200.kernels import (beam_reach, boresight_phi_host, make_args, pack_map,
+                                                           ring_table, table_slots)
+
+    B, S, nside = 2000, 1512, 1024
+    vec, bv, params, mp = _config2_like(B, S, nside, seed=9)
+    dev = torch.device("cuda")
+    to = lambda a: torch.from_numpy(np.ascontiguousarray(a)).to(dev)  # noqa: E731
+    p = [to(vec)] + [to(x) for x in params]
+    bore = to(boresight_phi_host(params[3]))
+    bvt = to(bv)
+    rec = pack_map(to(mp), "f64")
+    reach = beam_reach(vec, nside)
+    table = ring_table(nside, reach, dev)
+    interp = _native.BILINEAR if mode == "bilinear" else _native.NEAREST
+    est = table_slots(nside, reach)
+    assert est > 0
+    outs = []
+    for slots, tab in ((16, table), (0, table), (est, table), (1 << 20, table), (0, None)):
+        tod = torch.zeros((3, B), dtype=torch.float64, device=dev)
+        a = make_args(interp, nside, B, S, 3, 1, 2, p, np.float32, bore, bvt, rec, tod, table=tab)
+        a.tab_slots = slots
+        _native.check(_native.lib().todgpu_gather_accum(ctypes.byref(a), torch.cuda.current_stream().cuda_stream))
+        outs.append(tod.cpu().numpy())
+    for o in outs[1:]:
+        assert np.array_equal(o, outs[0])

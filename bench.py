@@ -383,10 +383,14 @@ def run_ours(args, dist):
     params_h = R._rotation_params(wl["rot"], wl["phi"], wl["theta"], wl["psis"])
     bore_h = boresight_phi_host(params_h[3])
     to = lambda a: torch.from_numpy(np.ascontiguousarray(a)).to(dev)  # noqa: E731
-    params = [to(beam.vec_orig)] + [to(p) for p in params_h]
+    from tod_generation_mapbased_beam_b200.kernels import beam_order, pack_map
+
+    # the beam's pixels in the library's gather order (as every beam-level entry
+    # point uploads them; only the order of the pixel sum changes)
+    order = beam_order(beam.vec_orig)
+    params = [to(beam.vec_orig[order])] + [to(p) for p in params_h]
     bore = to(bore_h)
-    bv = to(beam.beam_vals)
-    from tod_generation_mapbased_beam_b200.kernels import pack_map
+    bv = to(beam.beam_vals[order])
 
     sky = to(wl["sky"])
     # float64 map as float64 records {I, Q, U, 0}: the library's layout for the
@@ -585,7 +589,7 @@ def run_precision(args, dist, sky):
 
     from tod_generation_mapbased_beam_b200 import _native
     from tod_generation_mapbased_beam_b200 import workloads as W
-    from tod_generation_mapbased_beam_b200.kernels import gather_accum_angles, pack_map
+    from tod_generation_mapbased_beam_b200.kernels import beam_order, gather_accum_angles, pack_map
 
     dev = torch.device("cuda", dist.local)
     stream = torch.cuda.current_stream(dev)
@@ -594,8 +598,9 @@ def run_precision(args, dist, sky):
     B = args.samples
     th, ph, ps = W.spin_scan(B, 100.0, phi0=0.7 * dist.rank)
     ang = [torch.from_numpy(a).to(dev) for a in (th, ph, ps)]
-    vec = torch.from_numpy(beam.vec_orig.astype(np.float64)).to(dev)
-    bv = torch.from_numpy(beam.beam_vals).to(dev)
+    order = beam_order(beam.vec_orig)
+    vec = torch.from_numpy(beam.vec_orig.astype(np.float64)[order]).to(dev)
+    bv = torch.from_numpy(beam.beam_vals[order]).to(dev)
     interp = _native.BILINEAR if args.mode == "bilinear" else _native.NEAREST
     idx = torch.from_numpy(np.linspace(0, B - 1, 4096).astype(np.int64)).to(dev)
     out, subs = {}, {}

@@ -12,7 +12,7 @@ import torch
 from tod_generation_mapbased_beam_b200 import _native, autotune
 from tod_generation_mapbased_beam_b200 import workloads as W
 from tod_generation_mapbased_beam_b200.batched import DetectorBatch
-from tod_generation_mapbased_beam_b200.kernels import gather_accum_angles, pack_map
+from tod_generation_mapbased_beam_b200.kernels import beam_order, gather_accum_angles, pack_map
 
 pytestmark = pytest.mark.gpu
 
@@ -25,11 +25,14 @@ def small_config4():
 
 
 def _single(dets, sky, nside, interp):
+    """One gather per detector, its beam pixels in the order DetectorBatch
+    uploads them (kernels.beam_order)."""
     outs = []
     for d in dets:
+        o = beam_order(d["vec_orig"])
         tod = torch.zeros((3, len(d["theta"])), dtype=torch.float64, device="cuda")
-        gather_accum_angles(interp, d["vec_orig"], d["theta"], d["phi"], d["psi"], 0.0, 0.0, nside, sky,
-                            d["beam_vals"], tod, 1, 2)
+        gather_accum_angles(interp, np.asarray(d["vec_orig"])[o], d["theta"], d["phi"], d["psi"], 0.0, 0.0, nside,
+                            sky, np.asarray(d["beam_vals"])[o], tod, 1, 2)
         outs.append(tod.cpu().numpy())
     return outs
 

@@ -62,3 +62,31 @@ def test_chunked_parameter_preparation_bit_exact():
         got = [np.concatenate(f) for f in fields]
         for i, ref in enumerate(list(whole) + [bore]):
             assert np.array_equal(got[i], np.asarray(ref, np.float32).reshape(-1)), (step, i)
+
+
+def test_beam_order_is_a_local_permutation():
+    """The gather's beam-pixel order: a permutation whose consecutive pixels
+    are neighbours on the sky (Morton order in the plane of the beam), for a
+    pole-centred and for an offset beam."""
+    from tod_generation_mapbased_beam_b200.kernels import beam_order
+
+    beam = W.pole_gaussian_beam(30.0, 2048, 0.99, search_fwhm=1.5)
+    rot = np.array([[1.0, 0.0, 0.0], [0.0, np.cos(0.3), -np.sin(0.3)], [0.0, np.sin(0.3), np.cos(0.3)]])
+    for v in (beam.vec_orig.astype(np.float64), beam.vec_orig.astype(np.float64) @ rot.T):
+        o = beam_order(v)
+        assert np.array_equal(np.sort(o), np.arange(len(v)))
+
+        def span(u):
+            # median extent of a warp's 32 consecutive pixels, across the beam axis
+            c = u.mean(axis=0)
+            c /= np.linalg.norm(c)
+            e1 = np.cross(c, [1.0, 0.0, 0.0])
+            e1 /= np.linalg.norm(e1)
+            e2 = np.cross(c, e1)
+            xy = np.stack([u @ e1, u @ e2], -1)
+            return np.median([np.ptp(xy[k:k + 32], axis=0).max() for k in range(0, len(u) - 32, 32)])
+
+        # ring order strings a warp along an arc; the Morton order keeps it compact
+        assert span(v[o]) < 0.5 * span(v)
+        assert span(v[o]) < 12 * np.sqrt(4 * np.pi / (12 * 2048 ** 2))
+    assert list(beam_order(np.zeros((1, 3)))) == [0]

@@ -24,8 +24,8 @@ import torch
 
 from . import _native
 from ._device import require_cuda, stream_handle, to_device
-from .kernels import (PackedMap, _map_tensor, _ncomp, _row_stride, _set_map, beam_reach, pointing_buffers,
-                      pointing_params, ring_table, table_slots_for)
+from .kernels import (PackedMap, _map_tensor, _ncomp, _row_stride, _set_map, beam_order, beam_reach,
+                      pointing_buffers, pointing_params, ring_table, table_slots_for)
 
 
 class DetectorBatch:
@@ -48,9 +48,12 @@ class DetectorBatch:
         self.vec, self.beam, self.angles, self.out, self.centers = [], [], [], [], []
         self.tables = []
         for d in detectors:
-            vec = to_device(d["vec_orig"], np.float64).reshape(-1, 3)
+            # pixels in the gather's preferred order (neighbours on the sky next to
+            # each other; only the order of the pixel sums changes)
+            order = torch.from_numpy(beam_order(d["vec_orig"])).to(dev)
+            vec = to_device(d["vec_orig"], np.float64).reshape(-1, 3)[order].contiguous()
             self.vec.append(vec)
-            self.beam.append(to_device(d["beam_vals"], np.float32).reshape(-1))
+            self.beam.append(to_device(d["beam_vals"], np.float32).reshape(-1)[order].contiguous())
             ang = [to_device(d[k], np.float32).reshape(-1) for k in ("theta", "phi", "psi")]
             self.angles.append(ang)
             self.out.append(torch.zeros((self.C, ang[0].shape[0]), dtype=torch.float64, device=dev))

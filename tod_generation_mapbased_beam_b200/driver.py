@@ -33,7 +33,7 @@ import torch
 from . import _native
 from ._device import require_cuda
 from .kernels import beam_center_angles, gather_accum_angles
-from .tod_core import _cache, _INTERP, beam_tod_batch, component_slots, device_map
+from .tod_core import _INTERP, beam_tod_batch, component_slots, device_beam, device_map
 from .tod_rotations import precompute_rotation_vector_batch
 
 __all__ = ["load_scan_information", "open_scan_day", "DayRunner", "tod_exact_gen_batched",
@@ -164,9 +164,9 @@ class DayRunner:
             for data in self.beam_data.values():
                 comps = list(data["comp_indices"])
                 c_q, c_u = component_slots(comps)
+                vec, bv = device_beam(data["vec_orig"], data["beam_vals"], torch.float64)
                 self._entries.append(_Entry(
-                    comps, c_q, c_u, _cache.get(data["vec_orig"], torch.float64),
-                    _cache.get(data["beam_vals"], torch.float32), device_map(data, self.mp),
+                    comps, c_q, c_u, vec, bv, device_map(data, self.mp),
                     beam_center_angles(data["ra"], data["dec"]), _rows(len(comps), comps)))
 
     # -- reference pointing -------------------------------------------------

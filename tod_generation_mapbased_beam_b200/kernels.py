@@ -104,6 +104,45 @@ def _beam_reach(vec_orig, nside):
     return r + 3.0 / float(nside) + 2e-5
 
 
+def _spread16(a):
+    """The low 16 bits of a with a zero bit inserted after each."""
+    a = a & 0xFFFF
+    a = (a | (a << 8)) & 0x00FF00FF
+    a = (a | (a << 4)) & 0x0F0F0F0F
+    a = (a | (a << 2)) & 0x33333333
+    a = (a | (a << 1)) & 0x55555555
+    return a
+
+
+def beam_order(vec_orig):
+    """Order of a beam's pixels that puts neighbours on the sky next to each
+    other: the Morton (Z) order of their coordinates in the plane orthogonal to
+    the beam's mean direction, 16 bits per axis.  Consecutive pixels go to
+    neighbouring threads of a warp, whose stencils then share memory sectors
+    of the map (config 3: 16 sectors per gather request in the ring order of
+    the pixelised beam).  Only the order of the sum over beam pixels changes."""
+    v = vec_orig.detach().cpu().numpy() if is_tensor(vec_orig) else np.asarray(vec_orig)
+    v = np.asarray(v, np.float64).reshape(-1, 3)
+    n = v.shape[0]
+    if n < 2:
+        return np.arange(n, dtype=np.int64)
+    c = v.sum(axis=0)
+    nc = np.linalg.norm(c)
+    c = c / nc if nc > 0 else np.array([0.0, 0.0, 1.0])
+    a = np.zeros(3)
+    a[int(np.argmin(np.abs(c)))] = 1.0
+    e1 = np.cross(c, a)
+    e1 /= np.linalg.norm(e1)
+    e2 = np.cross(c, e1)
+    code = np.zeros(n, dtype=np.int64)
+    for shift, e in ((0, e1), (1, e2)):
+        x = v @ e
+        lo, hi = x.min(), x.max()
+        q = np.clip(((x - lo) / max(hi - lo, 1e-300) * 65535.0).astype(np.int64), 0, 65535)
+        code |= _spread16(q) << shift
+    return np.argsort(code, kind="stable")
+
+
 _TABLE_REACH = {}  # data_ptr of a cached ring table -> the reach it was built for
 
 

@@ -27,7 +27,7 @@ import torch
 
 from . import _native
 from ._device import require_cuda
-from .kernels import gather_accum_angles, pack_map
+from .kernels import beam_order, gather_accum_angles, pack_map
 from .tailnet import TailNet
 
 _INTERP = {"bilinear": _native.BILINEAR, "nearest": _native.NEAREST}
@@ -61,10 +61,13 @@ class LearnedTailTOD:
         self.main_map = main_map
         self.interp = _INTERP[interp]
         self.center = (float(center[0]), float(center[1]))
-        self.main_vec = torch.as_tensor(np.asarray(main.vec_orig, np.float64), device=self.device)
-        self.main_bv = torch.as_tensor(np.asarray(main.beam_vals, np.float32), device=self.device)
-        self.tail_vec = torch.as_tensor(np.asarray(tail.vec_orig, np.float64), device=self.device)
-        self.tail_bv = torch.as_tensor(np.asarray(tail.beam_vals, np.float32), device=self.device)
+        # beam pixels in the gather's preferred order (neighbours on the sky next
+        # to each other; only the order of the pixel sums changes)
+        mo, to_ = beam_order(main.vec_orig), beam_order(tail.vec_orig)
+        self.main_vec = torch.as_tensor(np.asarray(main.vec_orig, np.float64)[mo], device=self.device)
+        self.main_bv = torch.as_tensor(np.asarray(main.beam_vals, np.float32)[mo], device=self.device)
+        self.tail_vec = torch.as_tensor(np.asarray(tail.vec_orig, np.float64)[to_], device=self.device)
+        self.tail_bv = torch.as_tensor(np.asarray(tail.beam_vals, np.float32)[to_], device=self.device)
         self.tail_chunk = int(tail_chunk)
         self.net = None
         self.judged = None

@@ -1,4 +1,5 @@
-"""Batched detectors in one persistent launch (config 4 of the benchmark).
+"""Batched detectors in one persistent launch (e.g. 64 detectors, each with its
+own beam and a scan of its own length).
 
 :class:`DetectorBatch` holds, on the GPU, every detector's beam (vectors and
 weights), its scan angles and its (C, n) float64 output, and runs them all

@@ -119,8 +119,9 @@ def beam_order(vec_orig):
     other: the Morton (Z) order of their coordinates in the plane orthogonal to
     the beam's mean direction, 16 bits per axis.  Consecutive pixels go to
     neighbouring threads of a warp, whose stencils then share memory sectors
-    of the map (config 3: 16 sectors per gather request in the ring order of
-    the pixelised beam).  Only the order of the sum over beam pixels changes."""
+    of the map (a 30' beam pixelised at nside 4096 over an nside 2048 map made
+    16 sectors per gather request in its ring order).  Only the order of the
+    sum over beam pixels changes."""
     v = vec_orig.detach().cpu().numpy() if is_tensor(vec_orig) else np.asarray(vec_orig)
     v = np.asarray(v, np.float64).reshape(-1, 3)
     n = v.shape[0]

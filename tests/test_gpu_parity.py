@@ -492,3 +492,39 @@ def test_table_slots_change_speed_only(mode):
         outs.append(tod.cpu().numpy())
     for o in outs[1:]:
         assert np.array_equal(o, outs[0])
+
+
+def test_device_beam_order_and_drop_in_identity():
+    """Beams are uploaded once with their pixels in kernels.beam_order: the
+    cached device copy is that permutation of the host arrays, and the drop-in
+    equals a kernel-level gather given the same order bit for bit (and the
+    caller's order to the oracle bounds)."""
+    from tod_generation_mapbased_beam_b200 import _native
+    from tod_generation_mapbased_beam_b200 import tod_rotations as R
+    from tod_generation_mapbased_beam_b200 import workloads as W
+    from tod_generation_mapbased_beam_b200.kernels import beam_order, gather_accum
+
+    nside, B = 256, 3000
+    beam = W.pole_gaussian_beam(60.0, 512, 0.99, search_fwhm=1.5)
+    order = beam_order(beam.vec_orig)
+    vec, bv = tod_core.device_beam(beam.vec_orig, beam.beam_vals, torch.float32)
+    assert np.array_equal(vec.cpu().numpy(), beam.vec_orig[order])
+    assert np.array_equal(bv.cpu().numpy(), beam.beam_vals[order])
+    again = tod_core.device_beam(beam.vec_orig, beam.beam_vals, torch.float32)
+    assert again[0] is vec and again[1] is bv
+    th, ph, ps = W.spin_scan(B, 20.0, phi0=0.4)
+    rot, beta = R.precompute_rotation_vector_batch(beam.ra, beam.dec, ph, th)
+    psis = -beta + ps
+    sky = W.white_sky(nside, 12)
+    data = dict(vec_orig=beam.vec_orig, beam_vals=beam.beam_vals, comp_indices=[0, 1, 2], mp_stacked=sky,
+                ra=beam.ra, dec=beam.dec)
+    got = tod_core.beam_tod_batch(nside, None, data, rot, ph, th, psis, return_device=True).cpu().numpy()
+    params = R._rotation_params(rot, ph, th, psis)
+    for vec_in, bv_in, exact in ((beam.vec_orig[order], beam.beam_vals[order], True),
+                                 (beam.vec_orig, beam.beam_vals, False)):
+        tod = np.zeros((3, B))
+        gather_accum(_native.BILINEAR, vec_in, *params, nside, sky, bv_in, B, beam.S, tod, 1, 2)
+        if exact:
+            assert np.array_equal(got, tod)
+        else:
+            assert _rel(got, tod, 0.0) <= TOD_RTOL

@@ -2,7 +2,6 @@
 equals one gather per detector, bit for bit; CUDA-graph replay equals the
 eager launch; the tile size changes the schedule, not the result."""
 
-import ctypes
 import json
 
 import numpy as np

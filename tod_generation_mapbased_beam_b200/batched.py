@@ -18,15 +18,14 @@ one gather per detector (tests/test_gpu_batched.py checks bit-identity).
 
 from __future__ import annotations
 
-import ctypes
 
 import numpy as np
 import torch
 
 from . import _native
 from ._device import require_cuda, stream_handle, to_device
-from .kernels import (PackedMap, _map_tensor, _ncomp, _row_stride, _set_map, beam_order, beam_reach,
-                      pointing_buffers, pointing_params, ring_table, table_slots_for)
+from .kernels import (_map_tensor, _ncomp, _row_stride, _set_map, beam_order, beam_reach, pointing_buffers,
+                      pointing_params, ring_table, table_slots_for)
 
 
 class DetectorBatch:

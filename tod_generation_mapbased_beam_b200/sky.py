@@ -13,8 +13,6 @@ stream.
 
 from __future__ import annotations
 
-import ctypes
-
 import numpy as np
 import torch
 

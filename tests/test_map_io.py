@@ -171,3 +171,45 @@ def test_prepare_beam_data_and_load_sky(tmp_path):
     mp = driver.load_sky(folder + "sky.fits")
     assert len(mp) == 3 and all(m.dtype == np.float32 for m in mp)
     assert all(np.array_equal(m, s.astype(np.float32)) for m, s in zip(mp, sky))
+
+
+def _image_file(path, data_be, bitpix, extra_cards=()):
+    """A primary-HDU FITS image with the given big-endian data and cards."""
+    cards = [MI._card("SIMPLE", True), MI._card("BITPIX", bitpix), MI._card("NAXIS", data_be.ndim)]
+    for i, n in enumerate(reversed(data_be.shape)):
+        cards.append(MI._card(f"NAXIS{i + 1}", int(n)))
+    cards += [MI._card("CTYPE1", "RA---CAR"), MI._card("CTYPE2", "DEC--CAR"), MI._card("CDELT1", -0.05),
+              MI._card("CDELT2", 0.05), MI._card("CRPIX1", 3.0), MI._card("CRPIX2", 2.0)]
+    cards += list(extra_cards)
+    raw = data_be.tobytes()
+    with open(path, "wb") as f:
+        f.write(MI._header_bytes(cards))
+        f.write(raw)
+        f.write(MI._pad(len(raw)))
+
+
+def test_load_beam_scaled_integer_and_2d_images(tmp_path):
+    """BSCALE / BZERO integer images are scaled like FITS readers do; a 2-D
+    image gives map[0] = its first row, as the reference's map[0] does."""
+    vals = np.arange(20, dtype=np.int16).reshape(1, 4, 5)
+    _image_file(tmp_path / "i.fits", vals.astype(">i2"), 16, [MI._card("BSCALE", 0.5), MI._card("BZERO", 1.0)])
+    ra, dec, pm = MI.load_beam(str(tmp_path) + "/", "i.fits")
+    assert np.array_equal(pm, vals[0] * 0.5 + 1.0) and ra.shape == (4, 5)
+    flat = np.linspace(0, 1, 12).reshape(3, 4)
+    _image_file(tmp_path / "f.fits", flat.astype(">f4"), -32)
+    ra, dec, pm = MI.load_beam(str(tmp_path) + "/", "f.fits")
+    assert pm.shape == (4,) and np.array_equal(pm, flat[0].astype(np.float32))
+    # offsets: declination along rows, right ascension along columns (pixell's posmap order)
+    assert np.allclose(ra[:, 0], np.radians(0.05) * (np.arange(3) - 1))
+    assert np.allclose(dec[0], np.radians(-0.05) * (np.arange(4) - 2))
+
+
+@pytest.mark.parametrize("dtype", [np.float32, np.float64, np.int32, np.int64, np.int16])
+def test_map_column_types(tmp_path, dtype):
+    nside = 4
+    m = (np.arange(12 * nside * nside) % 97 - 40).astype(dtype)
+    p = str(tmp_path / "m.fits")
+    MI.write_map(p, m, dtype=dtype)
+    got = MI.read_map(p)
+    assert got.dtype == np.dtype(dtype) and np.array_equal(got, m)
+    assert MI.read_map(p, dtype=np.float64).dtype == np.float64

@@ -104,3 +104,17 @@ def test_table_slots_request():
     assert 900 < K.table_slots(1024, 0.0143) < 1200  # config 2: ~1.05 x 3 r^2 n^2 + 5 per ring, +10%
     assert K.table_slots(256, 0.05) == 0 and K.table_slots(256, 0.2) == 0
     assert K.table_slots_for(None, 1024) == 0
+
+
+def test_pointing_params_validation():
+    """todgpu_pointing_params checks its arguments before any CUDA call: a
+    negative count, a bad angle type and NULL arrays are rejected; no samples
+    is a no-op."""
+    lib = _native.lib()
+    p = ctypes.c_void_p(16)  # never dereferenced: every case fails (or returns) before use
+    args = lambda B, dt, ptr: [ptr, p, p, dt, B, 0.0, 0.0] + [p] * 6 + [None]  # noqa: E731
+    assert lib.todgpu_pointing_params(*args(-1, _native.F32, p)) == _native.ESHAPE
+    assert lib.todgpu_pointing_params(*args(4, 7, p)) == _native.EDTYPE
+    assert lib.todgpu_pointing_params(*args(4, _native.F64, None)) == _native.EINVAL
+    assert lib.todgpu_pointing_params(*args(0, _native.F32, None)) == 0
+    assert lib.todgpu_last_error_string()

@@ -5,22 +5,32 @@ Workload (config 2, plain method on GPU): HEALPix RING nside 1024 float64
 I/Q/U sky, circular Gaussian beam FWHM 30' at beam nside 2048 with a 0.99
 power cut (S = 1512 beam pixels), one 24 h batch of a 100 Hz spin scan
 (8.64e6 samples), one beam entry carrying I, Q and U (spin-2 on), bilinear
-interpolation (``--mode nearest`` for the other mode).
+interpolation (``--mode nearest`` makes nearest the headline mode).
 
 A step is one pass of the fused kernel over the whole batch.
 
 * ``value``: samples/s with the kernel inputs (float32 rotation parameters,
   boresight longitudes, beam, map) resident in HBM; the step zeroes the
   float64 (3, B) accumulator and runs the kernel.  Inputs (~1 GB) exceed L2.
-* ``e2e``: the same metric through the public drop-in
-  ``tod_core.beam_tod_batch`` with host numpy inputs (rot_vecs, phi, theta,
-  psis) -> float32 host dict: host parameter preparation, host->device copies,
-  kernel and device->host copy are all inside the timed region.
+* ``roofline``: the gather view of the kernel -- S x K stencil pixels of R =
+  32-byte float64 records per sample -- against the L2 read bandwidth
+  measured live by ``todgpu_l2_probe``.
+* ``parity``: both modes of the timed configuration (same beam order, same
+  map records, same float32 parameters) against the CPU oracle on a subset of
+  samples spread over the day; nearest-pixel identity by an index map.
+* ``nearest`` (or ``bilinear`` under ``--mode nearest``): the other mode,
+  timed on the same workload.
+* ``e2e``: the day driver with host float32 scan in and host float64 (3, n)
+  out, copies inside the timed region; ``e2e_drop_in``: the drop-in
+  ``tod_core.beam_tod_batch`` from host arrays.
 * ``cpu_baseline``: the CPU oracle (a C/OpenMP restatement of the reference's
   Numba kernel) on the host cores, on a bounded sample of the same workload.
+* ``mixed``, ``precision`` (config 3), ``batched`` (config 4), ``learned``
+  (config 5): the other forms, each as value, time and error only.
 
-``--impl reference`` times that CPU implementation as the benchmark itself
-(rank 0 only), on a bounded sample per step.
+``--impl reference`` times the CPU implementation as the benchmark itself
+(rank 0 only, bounded sample per step) on a sky built on the CPU: nothing of
+the GPU library is loaded in that arm.
 
 Multi-GPU (torchrun): each rank runs its own day of samples (weak scaling, no
 collective on the data path); timings are max-reduced over ranks.
@@ -47,10 +57,12 @@ sys.path.insert(0, ROOT)
 METRIC = "TOD samples/s, 1 B200: FP64 plain vs mixed/learned-tail at fixed RMS error"
 
 # FP64 flops per (sample, beam pixel) evaluation of the reference algorithm,
-# counted by ncu on the direct-evaluation path (TODGPU_FLAG_NO_TABLES) of the
-# config-2 workload: dadd + dmul + 2 * dfma per evaluation
-# (profiles/gather_accum_{bilinear,nearest}_config2.md).
-FLOPS_PER_EVAL = {"bilinear": 853.0, "nearest": 500.0}
+# counted by ncu (dadd + dmul + 2 * dfma) on the direct-evaluation path
+# (TODGPU_FLAG_NO_TABLES) of the config-2 workload.  The timed kernel takes
+# spin-2 angles from per-sample tables, so it executes fewer: the rate below
+# is reference-equivalent work per second, not pipe utilisation.
+REF_FLOPS_PER_EVAL = {"bilinear": 853.0, "nearest": 500.0}
+STENCIL = {"bilinear": 4, "nearest": 1}
 
 
 def parse_args():
@@ -63,6 +75,10 @@ def parse_args():
     p.add_argument("--samples", type=int, default=8_640_000)
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--no-parity", action="store_true", help="skip the oracle parity of the timed day")
+    p.add_argument("--parity-samples", type=int, default=200_000,
+                   help="samples of the timed day compared with the CPU oracle (spread over the day)")
+    p.add_argument("--no-other-mode", action="store_true", help="skip the timed leg of the other mode")
     p.add_argument("--no-mixed", action="store_true", help="skip the mixed-precision forms")
     p.add_argument("--no-learned", action="store_true", help="skip the learned-tail form (config 5)")
     p.add_argument("--no-precision", action="store_true", help="skip the nside 2048 precision form (config 3)")
@@ -75,6 +91,15 @@ def parse_args():
     p.add_argument("--cpu-seconds", type=float, default=10.0,
                    help="target CPU time of the bounded CPU-baseline sample")
     return p.parse_args()
+
+
+def g4(x):
+    """x rounded to 4 significant digits (keeps the JSON line short)."""
+    if x is None:
+        return None
+    if isinstance(x, (list, tuple)):
+        return [g4(v) for v in x]
+    return float(f"{float(x):.4g}")
 
 
 # ---------------------------------------------------------------------------
@@ -182,19 +207,24 @@ class ClockSampler:
 # workload
 # ---------------------------------------------------------------------------
 
-def make_workload(n_samples, rank):
+def _numpy_modules():
     from tod_generation_mapbased_beam_b200 import tod_rotations as R
     from tod_generation_mapbased_beam_b200 import workloads as W
 
+    return R, W
+
+
+def make_workload(n_samples, rank, gpu_sky=True):
+    """Config-2 workload of one rank.  The sky is synthesised on the GPU
+    (synfast-like: C_l^TT ~ (l+10)^-2 at 100 uK RMS, EE/BB at 10%/1%, seed 1);
+    with ``gpu_sky=False`` (the CPU arm) it is a seeded Gaussian sky of the
+    same RMS built on the CPU -- the CPU path's cost does not depend on the
+    sky's content, and that arm then loads nothing of the GPU library."""
+    R, W = _numpy_modules()
     beam = W.pole_gaussian_beam(30.0, 2048, 0.99, search_fwhm=1.5)
     # each rank scans its own day (weak scaling): shift the start longitude
     theta, phi, psi = W.spin_scan(n_samples, 100.0, phi0=0.7 * rank)
-    # synfast-like sky: C_l^TT ~ (l+10)^-2 at 100 uK RMS, EE/BB at 10%/1%, seed 1
-    # (synthesised on the GPU; a CPU-only run times the CPU path on a seeded
-    # Gaussian sky of the same RMS, which does not change its cost)
-    import torch
-
-    if torch.cuda.is_available():
+    if gpu_sky:
         from tod_generation_mapbased_beam_b200 import sky as SKY
 
         sky = SKY.synfast_iqu(1024, seed=1).cpu().numpy()
@@ -205,54 +235,35 @@ def make_workload(n_samples, rank):
     return dict(nside=1024, beam=beam, theta=theta, phi=phi, psi=psi, psis=psis, rot=rot, sky=sky)
 
 
-def map_footprint_bytes(wl, itemsize):
-    """Bytes of the map rows the day's scan can touch (the scan sweeps every
-    longitude, so whole rings between the extreme colatitudes +- beam radius)."""
-    nside = wl["nside"]
-    r = wl["beam"].radius + 2 * np.sqrt(4 * np.pi / (12 * nside * nside))
-    th_lo = max(0.0, float(wl["theta"].min()) - r)
-    th_hi = min(np.pi, float(wl["theta"].max()) + r)
-    zs = [np.cos(th_lo), np.cos(th_hi)]
-
-    def first_pix_of_ring(ir):
-        if ir < nside:
-            return 2 * ir * (ir - 1)
-        if ir <= 3 * nside:
-            return 2 * nside * (nside - 1) + (ir - nside) * 4 * nside
-        i2 = 4 * nside - ir
-        return 12 * nside * nside - 2 * i2 * (i2 + 1)
-
-    def ring_of(z):
-        az = abs(z)
-        if az > 2 / 3:
-            ir = int(nside * np.sqrt(3 * (1 - az)))
-            return ir if z > 0 else 4 * nside - ir - 1
-        return int(nside * (2 - 1.5 * z))
-
-    ir0 = max(1, ring_of(zs[0]))
-    ir1 = min(4 * nside - 1, ring_of(zs[1]) + 1)
-    npx = first_pix_of_ring(ir1) + (4 * nside) - first_pix_of_ring(ir0)
-    npx = min(npx, 12 * nside * nside)
-    return npx * 3 * itemsize
+def bench_config(args, S, world):
+    return {"workload": f"config2 plain FP64 {args.mode}: nside 1024 f64 I/Q/U sky (f64 records), 30' beam "
+                        f"@ nside 2048 0.99 cut, 100 Hz spin scan, one I/Q/U entry (spin-2)",
+            "samples_per_gpu": args.samples, "S": S, "mode": args.mode,
+            "l2": "inputs > L2 (~1 GB), no flush", "params": "reference float32 rotation parameters",
+            "parallelism": f"samples x{world}"}
 
 
 # ---------------------------------------------------------------------------
-# CPU (oracle) timing
+# CPU (oracle) timing and parity
 # ---------------------------------------------------------------------------
+
+def oracle_fn(mode):
+    import oracle
+
+    return oracle.gather_accum_fused if mode == "bilinear" else oracle.gather_accum_nearest
+
 
 def cpu_rate(wl, mode, target_seconds):
     """Samples/s of the CPU oracle on a bounded sample; returns (rate, n, threads)."""
-    import oracle
-    from tod_generation_mapbased_beam_b200 import tod_rotations as R
-
+    R, _ = _numpy_modules()
     threads = len(os.sched_getaffinity(0))
     beam = wl["beam"]
+    fn = oracle_fn(mode)
 
     def run(lo, n):
         sl = slice(lo, lo + n)
         params = R._rotation_params(wl["rot"][sl], wl["phi"][sl], wl["theta"][sl], wl["psis"][sl])
         tod = np.zeros((3, n))
-        fn = oracle.gather_accum_fused if mode == "bilinear" else oracle.gather_accum_nearest
         t0 = time.perf_counter()
         fn(beam.vec_orig, *params, wl["nside"], wl["sky"], beam.beam_vals, n, beam.S, tod, 1, 2,
            nthreads=threads)
@@ -268,8 +279,53 @@ def cpu_rate(wl, mode, target_seconds):
     return n / best, n, threads
 
 
+def index_map(npix, device):
+    """(2, npix) float64 map whose values identify the pixel: p and a hash of
+    p below 2^20.  Summed with unit beam weights, every TOD value is an exact
+    integer (below 2^53), so two engines agree on it exactly only if they
+    picked the same pixels."""
+    import torch
+
+    p = torch.arange(npix, dtype=torch.int64, device=device)
+    return torch.stack([p.double(), ((p * 2654435761) % 1048573).double()]).contiguous()
+
+
+def oracle_parity(wl, params_h, order, gpu_tod, mode, idx, nthreads):
+    """Max |GPU - oracle| / max |oracle| over the subset idx of the day, for
+    the timed kernel's inputs (the beam in the same pixel order)."""
+    beam = wl["beam"]
+    sub = [np.ascontiguousarray(p[idx]) for p in params_h]
+    ref = np.zeros((3, idx.size))
+    oracle_fn(mode)(beam.vec_orig[order], *sub, wl["nside"], wl["sky"], beam.beam_vals[order], idx.size,
+                    beam.S, ref, 1, 2, nthreads=nthreads)
+    scale = float(np.abs(ref).max())
+    return float(np.abs(gpu_tod - ref).max()) / scale
+
+
+def nearest_pixel_identity(wl, params_h, idx, nthreads, dev):
+    """Nearest pixels of the GPU kernel and the oracle on the subset idx: the
+    index map with unit beam weights, compared exactly."""
+    import torch
+
+    from tod_generation_mapbased_beam_b200 import _native
+    from tod_generation_mapbased_beam_b200.kernels import gather_accum
+
+    beam = wl["beam"]
+    n = idx.size
+    sub = [np.ascontiguousarray(p[idx]) for p in params_h]
+    ones = np.ones(beam.S, np.float32)
+    imap = index_map(12 * wl["nside"] ** 2, dev)
+    got = torch.zeros((2, n), dtype=torch.float64, device=dev)
+    gather_accum(_native.NEAREST, beam.vec_orig, *sub, wl["nside"], imap, ones, n, beam.S, got)
+    ref = np.zeros((2, n))
+    oracle_fn("nearest")(beam.vec_orig, *sub, wl["nside"], imap.cpu().numpy(), ones, n, beam.S, ref,
+                         nthreads=nthreads)
+    got = got.cpu().numpy()
+    return bool(np.array_equal(got, ref)), int(np.count_nonzero(got != ref))
+
+
 # ---------------------------------------------------------------------------
-# GPU timing
+# GPU timing helpers
 # ---------------------------------------------------------------------------
 
 def measured_peaks():
@@ -278,7 +334,7 @@ def measured_peaks():
         with open(path) as f:
             return json.load(f), "measured"
     except (OSError, ValueError):
-        return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0}, "fallback"
+        return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0, "bf16_tflops_sustained": 1400.0}, "fallback"
 
 
 def fp64_peak_tflops():
@@ -333,47 +389,39 @@ def l2_peak_gbs():
     return best
 
 
-def profiled_traffic(mode):
-    """dram bytes per launch recorded by the committed ncu summary, if any."""
-    path = os.path.join(ROOT, "profiles", f"gather_accum_{mode}_config2.md")
-    try:
-        for line in open(path):
-            if line.strip().startswith("dram_bytes_per_launch:"):
-                return float(line.split(":", 1)[1].strip())
-    except OSError:
-        pass
-    return None
+def _evt_ms(fn, stream):
+    import torch
+
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    fn()
+    e1.record(stream)
+    e1.synchronize()
+    return e0.elapsed_time(e1)
 
 
-def mixed_error_uk(wl, mode, kind, tod, cargs, margs, lib, stream, n_sub=2000):
-    """RMS / max error [uK] of a mixed form against the FP64 oracle on the
-    first n_sub samples (the same float32 parameters, the float64 map)."""
-    import oracle
-    from tod_generation_mapbased_beam_b200 import _native
-    from tod_generation_mapbased_beam_b200 import tod_rotations as R
+def _err_uk(a, b):
+    d = (a - b) * 1e6
+    return {"rms_uK": g4(np.sqrt((d ** 2).mean(axis=1))), "max_uK": g4(np.abs(d).max(axis=1))}
 
-    beam = wl["beam"]
-    sl = slice(0, n_sub)
-    params = R._rotation_params(wl["rot"][sl], wl["phi"][sl], wl["theta"][sl], wl["psis"][sl])
-    ref = np.zeros((3, n_sub))
-    fn = oracle.gather_accum_fused if mode == "bilinear" else oracle.gather_accum_nearest
-    fn(beam.vec_orig, *params, wl["nside"], wl["sky"], beam.beam_vals, n_sub, beam.S, ref, 1, 2,
-       nthreads=len(os.sched_getaffinity(0)))
-    tod.zero_()
-    _native.check(lib.todgpu_gather_accum(ctypes.byref(margs), stream.cuda_stream))
-    got = tod[:, :n_sub].cpu().numpy()
-    err = (got - ref) * 1e6
-    return {"rms_uK": float(np.sqrt(np.mean(err ** 2))), "max_uK": float(np.abs(err).max()),
-            "error_sample": f"{n_sub} samples vs FP64 oracle (same float32 parameters, float64 map)"}
 
+def gather_frac(B, S, mode, rec_bytes, ms, l2_peak):
+    gb = float(B) * S * STENCIL[mode] * rec_bytes / (ms / 1e3) / 1e9
+    return gb, gb / l2_peak
+
+
+# ---------------------------------------------------------------------------
+# our arm
+# ---------------------------------------------------------------------------
 
 def run_ours(args, dist):
     import torch
 
     from tod_generation_mapbased_beam_b200 import _native, tod_core
     from tod_generation_mapbased_beam_b200 import tod_rotations as R
-    from tod_generation_mapbased_beam_b200.kernels import (beam_reach, boresight_phi_host, make_args,
-                                                           ring_table)
+    from tod_generation_mapbased_beam_b200.kernels import (beam_order, beam_reach, boresight_phi_host, make_args,
+                                                           pack_map, ring_table)
 
     dev = torch.device("cuda", dist.local)
     torch.cuda.set_device(dev)
@@ -383,7 +431,6 @@ def run_ours(args, dist):
     params_h = R._rotation_params(wl["rot"], wl["phi"], wl["theta"], wl["psis"])
     bore_h = boresight_phi_host(params_h[3])
     to = lambda a: torch.from_numpy(np.ascontiguousarray(a)).to(dev)  # noqa: E731
-    from tod_generation_mapbased_beam_b200.kernels import beam_order, pack_map
 
     # the beam's pixels in the library's gather order (as every beam-level entry
     # point uploads them; only the order of the pixel sum changes)
@@ -391,29 +438,31 @@ def run_ours(args, dist):
     params = [to(beam.vec_orig[order])] + [to(p) for p in params_h]
     bore = to(bore_h)
     bv = to(beam.beam_vals[order])
-
     sky = to(wl["sky"])
     # float64 map as float64 records {I, Q, U, 0}: the library's layout for the
     # float64 path (packed on upload; TOD bit-identical to the planar map)
     sky_rec = pack_map(sky, "f64")
-    tod = torch.zeros((3, B), dtype=torch.float64, device=dev)
-    interp = _native.BILINEAR if args.mode == "bilinear" else _native.NEAREST
     table = None if args.no_tables else ring_table(nside, beam_reach(beam.vec_orig, nside), dev)
-    cargs = make_args(interp, nside, B, S, 3, 1, 2, params, np.float32, bore, bv, sky_rec, tod,
-                      table=table)
     lib = _native.lib()
     stream = torch.cuda.current_stream(dev)
+    modes = [args.mode] + ([] if args.no_other_mode else [m for m in STENCIL if m != args.mode])
+    interp = {"bilinear": _native.BILINEAR, "nearest": _native.NEAREST}
+    tods = {m: torch.zeros((3, B), dtype=torch.float64, device=dev) for m in modes}
+    cargs = {m: make_args(interp[m], nside, B, S, 3, 1, 2, params, np.float32, bore, bv, sky_rec, tods[m],
+                          table=table) for m in modes}
 
-    def step():
-        tod.zero_()
-        torch.cuda.nvtx.range_push("plain_step")
-        k0.record(stream)
-        _native.check(lib.todgpu_gather_accum(ctypes.byref(cargs), stream.cuda_stream))
-        k1.record(stream)
-        torch.cuda.nvtx.range_pop()
+    def launch(m):
+        _native.check(lib.todgpu_gather_accum(ctypes.byref(cargs[m]), stream.cuda_stream))
 
     k0 = torch.cuda.Event(enable_timing=True)
     k1 = torch.cuda.Event(enable_timing=True)
+
+    def step():
+        tods[args.mode].zero_()
+        k0.record(stream)
+        launch(args.mode)
+        k1.record(stream)
+
     for _ in range(args.warmup):
         step()
     torch.cuda.synchronize()
@@ -439,81 +488,100 @@ def run_ours(args, dist):
     kernel_ms = dist.max(statistics.mean(kern_ms))
     value = B * dist.world * args.steps / (total_ms / 1e3)
 
-    # roofline of the fused kernel: FP64-pipe bound.  Algorithmic work per
-    # (sample, beam pixel) evaluation = the FP64 flops of the reference
-    # algorithm executed directly on this GPU (ncu: dadd + dmul + 2 dfma on
-    # the direct-evaluation path); peak = FP64 FMA throughput measured now.
+    # roofline: the gather view of the kernel -- S x K stencil pixels of R = 32
+    # byte float64 records per sample -- against the L2 read bandwidth measured
+    # now.  Beside it: the reference-equivalent FP64 rate (ncu-counted flops of
+    # the reference algorithm on this GPU) against the FP64 FMA peak measured
+    # now, and the compulsory HBM bytes against the measured HBM peak.
     peaks, peak_src = measured_peaks()
-    evals = float(B) * S
-    flops_per_eval = FLOPS_PER_EVAL[args.mode]
-    fp64_peak = fp64_peak_tflops()
-    achieved = evals * flops_per_eval / (kernel_ms / 1e3) / 1e12
-    bytes_per_launch = (B * (4 * 11 + 8 * 3 * 2) + S * 16 + map_footprint_bytes(wl, 8))
-    hbm_achieved = bytes_per_launch / (kernel_ms / 1e3) / 1e9
-    # the gather view: S x K stencil pixels of R = 32-byte float64 records per
-    # sample (K = 4 bilinear, 1 nearest), against the L2 read bandwidth
-    # measured now -- served mostly from L1, so not the bound of this kernel
-    gather_bytes = float(B) * S * (4 if args.mode == "bilinear" else 1) * 32
-    gather_gbs = gather_bytes / (kernel_ms / 1e3) / 1e9
     l2_peak = l2_peak_gbs()
-    roofline = {"bound": "fp64", "achieved": round(achieved, 3), "peak": round(fp64_peak, 3),
-                "unit": "TFLOP/s", "frac": round(achieved / fp64_peak, 4),
-                "traffic": profiled_traffic(args.mode),
-                "peak_source": "measured now (todgpu_fp64_probe: 8 independent FMA chains/thread)",
-                "algorithmic_flops_per_eval": flops_per_eval,
-                "evals_per_launch": int(evals), "kernel": "gather_accum_kernel",
-                "kernel_ms": round(kernel_ms, 3),
-                "hbm": {"achieved": round(hbm_achieved, 2), "peak": peaks["hbm_gbs"], "unit": "GB/s",
-                        "frac": round(hbm_achieved / peaks["hbm_gbs"], 5),
-                        "algorithmic_bytes_per_launch": int(bytes_per_launch),
-                        "peak_source": peak_src},
-                "gather": {"achieved": round(gather_gbs, 1), "peak": round(l2_peak, 1), "unit": "GB/s",
-                           "frac": round(gather_gbs / l2_peak, 4),
-                           "bytes_per_sample": int(gather_bytes / B),
-                           "peak_source": "measured now (todgpu_l2_probe: 16-byte L1-bypassing loads over "
-                                          "64 MiB)",
-                           "note": "logical stencil gathers; 93% are L1 hits, so this is not the bound"}}
+    g_gbs, g_frac = gather_frac(B, S, args.mode, 32, kernel_ms, l2_peak)
+    fp64_peak = fp64_peak_tflops()
+    ref_tflops = float(B) * S * REF_FLOPS_PER_EVAL[args.mode] / (kernel_ms / 1e3) / 1e12
+    hbm_bytes = B * (4 * 11 + 8 * 3 * 2) + S * 16
+    roofline = {"bound": "l2", "achieved": g4(g_gbs), "peak": g4(l2_peak), "unit": "GB/s", "frac": g4(g_frac),
+                "traffic": None, "kernel": "gather_accum_kernel", "kernel_ms": g4(kernel_ms),
+                "bytes_per_sample": S * STENCIL[args.mode] * 32,
+                "peak_source": "todgpu_l2_probe, measured in this run",
+                "ref_equiv_fp64_tflops": g4(ref_tflops), "fp64_peak_tflops": g4(fp64_peak),
+                "ref_equiv_fp64_frac": g4(ref_tflops / fp64_peak),
+                "hbm_frac": g4(hbm_bytes / (kernel_ms / 1e3) / 1e9 / peaks["hbm_gbs"]),
+                "hbm_peak_source": peak_src}
+    result = {"value": value, "ms_per_step": total_ms / args.steps, "roofline": roofline, "clocks": clk,
+              "gpu_launches": args.steps}
 
-    result = {"value": value, "ms_per_step": total_ms / args.steps, "roofline": roofline,
-              "clocks": clk, "gpu_launches": args.steps}
+    # the other mode on the same workload (same buffers, its own output)
+    for m in modes[1:]:
+        launch(m)
+        torch.cuda.synchronize()
+        times = []
+        for _ in range(args.steps):
+            tods[m].zero_()
+            times.append(_evt_ms(lambda: launch(m), stream))
+        ms = dist.max(statistics.mean(times))
+        _, fr = gather_frac(B, S, m, 32, ms, l2_peak)
+        result[m] = {"value": g4(B * dist.world / (ms / 1e3)), "kernel_ms": g4(ms), "gather_frac": g4(fr)}
+
+    # parity of the timed day: both modes against the CPU oracle on a subset
+    # spread over the day (same float32 parameters, same beam order, the
+    # float64 map), and the nearest pixels compared exactly by an index map
+    if not args.no_parity and dist.rank == 0:
+        t0 = time.perf_counter()
+        nthreads = len(os.sched_getaffinity(0))
+        n_sub = min(args.parity_samples, B)
+        idx = np.unique(np.linspace(0, B - 1, n_sub).astype(np.int64))
+        par = {"samples": int(idx.size), "of": B, "spread": "evenly over the day"}
+        idx_d = to(idx)
+        for m in modes:
+            rel = oracle_parity(wl, params_h, order, tods[m][:, idx_d].cpu().numpy(), m, idx, nthreads)
+            par[f"rel_err_{m}"] = g4(rel)
+        if "nearest" in modes:
+            same, ndiff = nearest_pixel_identity(wl, params_h, idx, nthreads, dev)
+            par["nearest_pixels_identical"] = same
+            if not same:
+                par["nearest_pixel_sums_differing"] = ndiff
+        par["tolerance"] = 1e-12
+        par["seconds"] = g4(time.perf_counter() - t0)
+        result["parity"] = par
 
     # mixed precision forms on the same workload: packed float32 / bfloat16
     # records, float32 spin-2 table, float32 Kahan sum, float64 decisions;
     # error against the FP64 oracle on a bounded subset of samples
     if not args.no_mixed:
         mixed = {}
+        tod = tods[args.mode]
         tod_rec = tod.clone()  # the float64 result of the last timed step
+        sub_ref = None
+        if dist.rank == 0 and not args.no_cpu_baseline:
+            n_sub = 2000
+            sub = [p[:n_sub] for p in params_h]
+            sub_ref = np.zeros((3, n_sub))
+            oracle_fn(args.mode)(beam.vec_orig, *sub, nside, wl["sky"], beam.beam_vals, n_sub, S, sub_ref, 1, 2,
+                                 nthreads=len(os.sched_getaffinity(0)))
         for kind in ("planar_f64", "f32", "bf16"):
             pm = sky if kind == "planar_f64" else pack_map(sky, kind)
-            margs = make_args(interp, nside, B, S, 3, 1, 2, params, np.float32, bore, bv, pm, tod,
+            margs = make_args(interp[args.mode], nside, B, S, 3, 1, 2, params, np.float32, bore, bv, pm, tod,
                               table=table)
             for _ in range(2):
                 _native.check(lib.todgpu_gather_accum(ctypes.byref(margs), stream.cuda_stream))
             torch.cuda.synchronize()
-            m0 = torch.cuda.Event(enable_timing=True)
-            m1 = torch.cuda.Event(enable_timing=True)
-            m0.record(stream)
+            times = []
             for _ in range(args.steps):
                 tod.zero_()
-                _native.check(lib.todgpu_gather_accum(ctypes.byref(margs), stream.cuda_stream))
-            m1.record(stream)
-            m1.synchronize()
-            mms = dist.max(m0.elapsed_time(m1) / args.steps)
-            entry = {"value": B * dist.world / (mms / 1e3), "ms_per_step": mms,
-                     "map": {"planar_f64": "planar float64 (C, N), the reference's mp_stacked",
-                             "f32": "packed f32 records (16 B/pixel)", "bf16": "packed bf16 records (8 B/pixel)"}[kind]}
-            # the gather view for this map layout: S x K stencil pixels of R bytes
-            # (planar float64: three 8-byte reads per pixel) against the L2 bandwidth
+                times.append(_evt_ms(lambda: _native.check(
+                    lib.todgpu_gather_accum(ctypes.byref(margs), stream.cuda_stream)), stream))
+            mms = dist.max(statistics.mean(times))
             rec = {"planar_f64": 24, "f32": 16, "bf16": 8}[kind]
-            gb = float(B) * S * (4 if args.mode == "bilinear" else 1) * rec / (mms / 1e3) / 1e9
-            entry["gather"] = {"bytes_per_sample": S * (4 if args.mode == "bilinear" else 1) * rec,
-                               "achieved": round(gb, 1), "peak": round(l2_peak, 1), "unit": "GB/s",
-                               "frac": round(gb / l2_peak, 4)}
+            _, fr = gather_frac(B, S, args.mode, rec, mms, l2_peak)
+            entry = {"value": g4(B * dist.world / (mms / 1e3)), "gather_frac": g4(fr)}
             if kind == "planar_f64":
-                entry["bit_identical_to_value"] = bool(torch.equal(tod, tod_rec))
-            elif dist.rank == 0 and not args.no_cpu_baseline:
-                entry.update(mixed_error_uk(wl, args.mode, kind, tod, cargs, margs, lib, stream))
+                entry["bit_identical"] = bool(torch.equal(tod, tod_rec))
+            elif sub_ref is not None:
+                err = (tod[:, :sub_ref.shape[1]].cpu().numpy() - sub_ref) * 1e6
+                entry["rms_uK"] = g4(float(np.sqrt(np.mean(err ** 2))))
+                entry["max_uK"] = g4(float(np.abs(err).max()))
             mixed[kind] = entry
+            del pm
         result["mixed"] = mixed
 
     # end to end with host buffers: the day driver (host float32 scan in,
@@ -541,52 +609,33 @@ def run_ours(args, dist):
         assert day.shape == (3, B)
         result["e2e"] = {"value": B * dist.world * args.steps / e2e_s, "unit": "samples/s",
                          "h2d_bytes_per_step": int(B * 3 * 4), "d2h_bytes_per_step": int(B * 3 * 8),
-                         "api": "driver.DayRunner.run: host float32 (theta, phi, psi) -> host "
-                                "float64 tod_day (3, n); rotation derived on the GPU in FP64"}
+                         "api": "driver.DayRunner.run: host f32 (theta, phi, psi) -> host f64 tod_day (3, n)"}
         drop_s, res = timed(lambda: tod_core.beam_tod_batch(nside, None, data, wl["rot"], wl["phi"],
                                                             wl["theta"], wl["psis"],
                                                             interp_mode=args.mode))
         assert res[0].shape == (B,)
-        result["e2e_drop_in"] = {"value": B * dist.world * args.steps / drop_s, "unit": "samples/s",
-                                 "h2d_bytes_per_step": int(B * (4 * 10 + 4)),
-                                 "d2h_bytes_per_step": int(B * 3 * 4),
-                                 "api": "tod_core.beam_tod_batch: host rot_vecs/angles in (host "
-                                        "float32 parameter prep as the reference), float32 dict out"}
+        result["e2e_drop_in"] = {"value": g4(B * dist.world * args.steps / drop_s),
+                                 "h2d_bytes_per_step": int(B * (4 * 10 + 4)), "d2h_bytes_per_step": int(B * 3 * 4)}
 
     if not args.no_cpu_baseline and dist.rank == 0:
         rate, n, threads = cpu_rate(wl, args.mode, args.cpu_seconds)
-        result["cpu_baseline"] = {"value": rate, "unit": "samples/s", "cores": threads,
-                                  "kind": "port",
-                                  "sample": f"{n} consecutive samples of the same workload "
-                                            f"(S={S}, nside {nside}), C/OpenMP oracle, best of 2"}
+        result["cpu_baseline"] = {"value": g4(rate), "unit": "samples/s", "cores": threads, "kind": "port",
+                                  "sample": f"{n} consecutive samples (S={S}, nside {nside}), C/OpenMP oracle, "
+                                            "best of 2"}
     return result, B, S
-
-
-def _evt_ms(fn, stream):
-    import torch
-
-    e0 = torch.cuda.Event(enable_timing=True)
-    e1 = torch.cuda.Event(enable_timing=True)
-    e0.record(stream)
-    fn()
-    e1.record(stream)
-    e1.synchronize()
-    return e0.elapsed_time(e1)
-
-
-def _err_uk(a, b):
-    d = (a - b) * 1e6
-    return {"rms_uK": np.sqrt((d ** 2).mean(axis=1)).tolist(), "max_uK": np.abs(d).max(axis=1).tolist()}
 
 
 def run_precision(args, dist, sky):
     """Precision form (config 3): nside 2048 synfast-like sky (seed 2) as
-    packed float32 and bfloat16 records, 30' beam at nside 4096 with a 0.999
-    cut, 8.64e6 scan samples with the rotation derived on the device in
-    float64; one timed launch per form (each ~4 s) after one warm-up, errors
-    on 4096 samples against the float64 path on the same inputs."""
+    float64, packed float32 and bfloat16 records, 30' beam at nside 4096 with
+    a 0.999 cut, 8.64e6 scan samples with the rotation derived on the device
+    in float64; one timed launch per form after one warm-up.  Errors on a
+    subset of samples spread over the day against the FP64 CPU oracle run of
+    the same inputs (pointing angles -> float64 rotation parameters -> float64
+    gather of the float64 map)."""
     import torch
 
+    import oracle
     from tod_generation_mapbased_beam_b200 import _native
     from tod_generation_mapbased_beam_b200 import workloads as W
     from tod_generation_mapbased_beam_b200.kernels import beam_order, gather_accum_angles, pack_map
@@ -599,10 +648,14 @@ def run_precision(args, dist, sky):
     th, ph, ps = W.spin_scan(B, 100.0, phi0=0.7 * dist.rank)
     ang = [torch.from_numpy(a).to(dev) for a in (th, ph, ps)]
     order = beam_order(beam.vec_orig)
-    vec = torch.from_numpy(beam.vec_orig.astype(np.float64)[order]).to(dev)
-    bv = torch.from_numpy(beam.beam_vals[order]).to(dev)
+    vec64 = beam.vec_orig.astype(np.float64)[order]
+    bv_h = beam.beam_vals[order]
+    vec = torch.from_numpy(vec64).to(dev)
+    bv = torch.from_numpy(bv_h).to(dev)
     interp = _native.BILINEAR if args.mode == "bilinear" else _native.NEAREST
-    idx = torch.from_numpy(np.linspace(0, B - 1, 4096).astype(np.int64)).to(dev)
+    n_sub = 8192
+    idx = np.linspace(0, B - 1, n_sub).astype(np.int64)
+    idx_d = torch.from_numpy(idx).to(dev)
     out, subs = {}, {}
     for kind in ("f64", "f32", "bf16"):
         mp = pack_map(sky, kind)
@@ -614,24 +667,25 @@ def run_precision(args, dist, sky):
 
         launch()
         ms = dist.max(_evt_ms(launch, stream))
-        subs[kind] = tod[:, idx].cpu().numpy()
+        subs[kind] = tod[:, idx_d].cpu().numpy()
         rec = {"f64": 32, "f32": 16, "bf16": 8}[kind]
-        kk = 4 if args.mode == "bilinear" else 1
-        gb = float(B) * beam.S * kk * rec / (ms / 1e3) / 1e9
-        out[kind] = {"value": B * dist.world / (ms / 1e3), "ms_per_step": ms,
-                     "map": {"f64": "packed f64 records (32 B/pixel; TOD bit-identical to the planar "
-                                    "float64 map)", "f32": "packed f32 records (16 B/pixel)",
-                             "bf16": "packed bf16 records (8 B/pixel)"}[kind],
-                     "gather": {"bytes_per_sample": beam.S * kk * rec, "achieved": round(gb, 1),
-                                "peak": round(l2_peak, 1), "unit": "GB/s", "frac": round(gb / l2_peak, 4)}}
+        _, fr = gather_frac(B, beam.S, args.mode, rec, ms, l2_peak)
+        out[kind] = {"value": g4(B * dist.world / (ms / 1e3)), "ms": g4(ms), "gather_frac": g4(fr)}
         del tod, mp
-    for kind in ("f32", "bf16"):
-        out[kind].update(_err_uk(subs[kind], subs["f64"]))
-    return {"workload": f"config3 precision form, {args.mode}: nside 2048 synfast-like sky (seed 2), 30' "
-                        f"beam @ nside 4096, 0.999 cut (S={beam.S}), 100 Hz scan, angles (FP64 rotation "
-                        "on the device)", "samples_per_gpu": B, "S": beam.S, "forms": out,
-            "error_reference": "float64 map, same kernel and pointing (the FP64 path, within 1e-10 of "
-                               "the FP64 CPU oracle in the tests); 4096 samples spread over the day"}
+    if dist.rank == 0 and not args.no_cpu_baseline:
+        t0 = time.perf_counter()
+        rv, beta = oracle.rotation_vectors_f64(0.0, 0.0, ph[idx], th[idx])
+        prm = oracle.rotation_params_f64(rv, ph[idx], th[idx], np.asarray(ps[idx], np.float64) - beta)
+        ref = np.zeros((3, n_sub))
+        oracle_fn(args.mode)(vec64, *prm, 2048, sky.cpu().numpy(), bv_h, n_sub, beam.S, ref, 1, 2,
+                             nthreads=len(os.sched_getaffinity(0)), f64=True)
+        for kind in ("f64", "f32", "bf16"):
+            out[kind].update(_err_uk(subs[kind], ref))
+        oracle_s = time.perf_counter() - t0
+    else:
+        oracle_s = None
+    return {"S": beam.S, "forms": out, "error_vs": f"FP64 CPU oracle, {n_sub} samples spread over the day",
+            "oracle_seconds": g4(oracle_s)}
 
 
 def run_batched(args, dist, sky):
@@ -659,22 +713,17 @@ def run_batched(args, dist, sky):
     torch.cuda.synchronize()
     times = [_evt_ms(batch.run, stream) for _ in range(args.steps)]
     ms = dist.max(statistics.mean(times))
-    n, evals = batch.n_samples, batch.n_evals
+    n = batch.n_samples
 
     def loop():
-        for d, vec, bvt, angs, o in zip(dets, batch.vec, batch.beam, batch.angles, batch.out):
+        for vec, bvt, angs, o in zip(batch.vec, batch.beam, batch.angles, batch.out):
             o.zero_()
             gather_accum_angles(batch.interp, vec, *angs, 0.0, 0.0, 2048, pm, bvt, o, c_q=1, c_u=2)
 
-    loop_ms = dist.max(_evt_ms(loop, stream))
+    loop_ms = dist.max(statistics.mean(_evt_ms(loop, stream) for _ in range(2)))
     batch.release()
-    return {"workload": f"config4 batched, {args.mode}: {len(dets)} detectors, own beams (S "
-                        f"{min(v.shape[0] for v in batch.vec)}-{max(v.shape[0] for v in batch.vec)}), "
-                        "scans log-uniform 1e5-9e6 samples, nside 2048 packed f32 sky",
-            "value": n * dist.world / (ms / 1e3), "unit": "samples/s", "samples_per_gpu": n,
-            "evals_per_s": evals * dist.world / (ms / 1e3), "ms_per_step": ms, "tile": batch.tile,
-            "autotune_seconds": tune_s, "graph": True,
-            "per_detector_launches_value": n * dist.world / (loop_ms / 1e3)}
+    return {"value": g4(n * dist.world / (ms / 1e3)), "ms": g4(ms), "samples": n, "tile": batch.tile,
+            "per_detector_value": g4(n * dist.world / (loop_ms / 1e3)), "autotune_s": g4(tune_s)}
 
 
 def run_learned(args, dist, sky):
@@ -684,8 +733,8 @@ def run_learned(args, dist, sky):
     the power replaced by the Fourier-feature network, trained here on
     plain-method tail targets at uniform pointings (seed 6).  Throughput over
     the config-2 scan (8.64e6 samples at 100 Hz) against the plain float64
-    path on the whole beam; errors on 4096 held-out scan samples against the
-    plain float64 path, with the tail dropped for comparison."""
+    path on the whole beam; errors per Stokes component on 4096 held-out scan
+    samples against the plain float64 path, with the tail dropped beside it."""
     import torch
 
     from tod_generation_mapbased_beam_b200 import learned as L
@@ -707,13 +756,11 @@ def run_learned(args, dist, sky):
     main_ms, net_ms = [], []
     for i in range(args.warmup + args.steps):
         tod.zero_()
-        torch.cuda.nvtx.range_push("learned_form")
         ev[0].record(stream)
         lt.main_lobe(*scan, tod)
         ev[1].record(stream)
         lt.learned_tail(*scan, tod)
         ev[2].record(stream)
-        torch.cuda.nvtx.range_pop()
         ev[2].synchronize()
         if i >= args.warmup:
             main_ms.append(ev[0].elapsed_time(ev[1]))
@@ -723,46 +770,36 @@ def run_learned(args, dist, sky):
     sub = [a[:2048] for a in held]
     lt.full_plain(*sub)
     torch.cuda.synchronize()
-    p0 = torch.cuda.Event(enable_timing=True)
-    p1 = torch.cuda.Event(enable_timing=True)
-    p0.record(stream)
-    lt.full_plain(*sub)
-    p1.record(stream)
-    p1.synchronize()
-    plain_rate = 2048 / (dist.max(p0.elapsed_time(p1)) / 1e3)
+    plain_ms = dist.max(_evt_ms(lambda: lt.full_plain(*sub), stream))
+    plain_rate = 2048 / (plain_ms / 1e3)
     value = B * dist.world / (step_ms / 1e3)
     F, H, D, O = lt.net.dims
     flops = 2.0 * (7 * F + 2 * F * H + (D - 1) * H * H + O * H)
-    peaks, peak_src = measured_peaks()
+    peaks, _ = measured_peaks()
     net_tflops = B * flops / (net_ms_mean / 1e3) / 1e12
-    bf16_peak = peaks.get("bf16_tflops", 1590.0)
+    peak = peaks.get("bf16_tflops_sustained", peaks.get("bf16_tflops", 1400.0))
     return {
-        "workload": "config5 learned tail: nside 2048 f64 synfast-like sky (seed 2); beam = 30' Gaussian "
-                    f"main lobe within 45' ({main.S} px, exact, packed f32 map + Kahan) + 10-20 deg annulus "
-                    f"({tail.S} px, 1% power, r^-3 x (1 + sum_m<=8 a_m cos(m phi + phi_m)), seed 5) replaced "
-                    "by the network; config-2 scan",
-        "value": value, "unit": "samples/s", "samples_per_gpu": B, "ms_per_step": step_ms,
-        "plain_fp64_value": plain_rate, "plain_fp64_sample": "2048 held-out scan samples, whole beam "
-                                                            "(main + tail) by the float64 gather",
-        "speedup_vs_plain_fp64": value / (plain_rate * dist.world),
-        "error_vs_plain_fp64": judged["learned"], "error_tail_dropped": judged["dropped"],
-        "tail_rms_uK": judged["tail_rms_uK"], "surrogate_error": judged["surrogate"],
-        "budget_uK": judged["budget_uK"], "within_budget": bool(judged["use_surrogate"]),
-        "judge_samples": judged["samples"],
-        "main_lobe_ms": statistics.mean(main_ms), "network_ms": net_ms_mean,
-        "network": {"dims": {"n_freq": F, "width": H, "depth": D, "n_out": O}, "flops_per_sample": flops,
-                    "achieved": round(net_tflops, 2), "unit": "TFLOP/s", "peak": bf16_peak,
-                    "frac": round(net_tflops / bf16_peak, 4),
-                    "peak_source": f"bf16 dense GEMM burst ({peak_src}); hidden layers on mma.sync bf16"},
-        "training": dict(info, sigma=list(lt.net.sigma)),
+        "value": g4(value), "ms": g4(step_ms), "plain_fp64_value": g4(plain_rate),
+        "speedup_vs_plain_fp64": g4(value / (plain_rate * dist.world)),
+        "err_rms_uK": g4(judged["learned"]["rms_uK"]), "dropped_rms_uK": g4(judged["dropped"]["rms_uK"]),
+        "err_max_uK": g4(judged["learned"]["max_uK"]), "budget_uK": 0.1,
+        "within_budget_per_component": bool(judged["use_surrogate"]),
+        "dropped_within_budget": bool(max(judged["dropped"]["rms_uK"]) <= 0.1),
+        "main_ms": g4(statistics.mean(main_ms)), "net_ms": g4(net_ms_mean),
+        "net_tflops": g4(net_tflops), "net_frac_bf16_sustained": g4(net_tflops / peak),
+        "n_train": info["n_train"], "target_s": g4(info["target_seconds"]), "train_s": g4(info["train_seconds"]),
     }
 
+
+# ---------------------------------------------------------------------------
+# the CPU arm
+# ---------------------------------------------------------------------------
 
 def run_reference(args):
     rank, world, _ = dist_env()
     if rank != 0:
         return None
-    wl = make_workload(min(args.samples, 2_000_000), 0)
+    wl = make_workload(min(args.samples, 2_000_000), 0, gpu_sky=False)
     rates = []
     per_step = max(2.0, 120.0 / max(1, args.steps + args.warmup))
     for i in range(args.warmup + args.steps):
@@ -771,31 +808,26 @@ def run_reference(args):
             rates.append((rate, n))
     value = statistics.mean(r for r, _ in rates)
     n = rates[-1][1]
-    return {"impl": "reference", "value": value, "threads": threads, "n": n, "S": wl["beam"].S}
+    return {"value": value, "threads": threads, "n": n, "S": wl["beam"].S}
 
 
 def main():
     args = parse_args()
     base = {"metric": METRIC, "unit": "samples/s", "higher_is_better": True, "steps": args.steps,
             "warmup": args.warmup, "vs_baseline": None, "dtype": "f64",
-            "data": "synthetic: seeded 100 Hz spin scan, pole-centred Gaussian beam, seeded "
-                    "synfast-like I/Q/U sky (GPU alm2map, C_l^TT ~ (l+10)^-2, 100 uK RMS)"}
-    config = {"workload": f"config2 plain FP64, {args.mode}: nside 1024 f64 I/Q/U sky (float64 records), 30' FWHM "
-                          f"beam @ nside 2048 0.99 cut, 100 Hz spin scan, one beam entry (I,Q,U; spin-2)",
-              "samples_per_gpu": args.samples, "mode": args.mode,
-              "l2": "inputs larger than L2 (params+map ~1 GB), no flush needed",
-              "params": "float32 reference-typed rotation parameters"}
+            "data": "synthetic: seeded 100 Hz spin scan, pole-centred Gaussian beam, seeded synfast-like "
+                    "I/Q/U sky (GPU alm2map; the CPU arm a seeded Gaussian sky of the same RMS)"}
     if args.impl == "reference":
         r = run_reference(args)
         if r is None:
             return
-        config["samples_per_gpu"] = r["n"]
         line = dict(base, impl="reference", value=r["value"], n_gpus=args.gpus,
-                    ms_per_step=r["n"] / r["value"] * 1e3, scaling="weak", config=config,
+                    ms_per_step=r["n"] / r["value"] * 1e3, scaling="weak",
+                    config=bench_config(args, r["S"], args.gpus),
                     cpu_baseline={"value": r["value"], "unit": "samples/s", "cores": r["threads"],
                                   "kind": "port",
-                                  "sample": f"{r['n']} samples per step (S={r['S']}), C/OpenMP "
-                                            "restatement of the reference Numba kernel"},
+                                  "sample": f"{r['n']} samples per step of the same day, C/OpenMP restatement "
+                                            "of the reference Numba kernel, CPU-built sky"},
                     e2e={"value": r["value"], "unit": "samples/s", "h2d_bytes_per_step": 0,
                          "d2h_bytes_per_step": 0})
         print(json.dumps(line))
@@ -809,10 +841,8 @@ def main():
         from tod_generation_mapbased_beam_b200 import sky as SKY
 
         torch.cuda.empty_cache()
-        t0 = time.perf_counter()
         sky2048 = SKY.synfast_iqu(2048, seed=2)  # configs 3-5
         torch.cuda.synchronize()
-        res["sky2048_seconds"] = time.perf_counter() - t0
         if not args.no_precision:
             res["precision"] = run_precision(args, dist, sky2048)
         if not args.no_batched:
@@ -822,15 +852,13 @@ def main():
         del sky2048
     if dist.rank == 0:
         line = dict(base, value=res["value"], n_gpus=dist.world, ms_per_step=res["ms_per_step"],
-                    scaling="weak", config=dict(config, S=S, parallelism=f"samples x{dist.world}"),
-                    roofline=res["roofline"], gpu_launches=res["gpu_launches"],
-                    clocks=res["clocks"])
-        for key in ("e2e", "e2e_drop_in", "mixed", "precision", "batched", "learned", "sky2048_seconds"):
+                    scaling="weak", config=bench_config(args, S, dist.world), roofline=res["roofline"],
+                    gpu_launches=res["gpu_launches"], clocks=res["clocks"])
+        for key in ("cpu_baseline", "e2e", "parity", "nearest", "bilinear", "e2e_drop_in", "mixed", "precision",
+                    "batched", "learned"):
             if key in res:
                 line[key] = res[key]
-        if "cpu_baseline" in res:
-            line["cpu_baseline"] = res["cpu_baseline"]
-        print(json.dumps(line))
+        print(json.dumps(line, separators=(",", ":")))
     dist.close()
 
 

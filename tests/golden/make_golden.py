@@ -1,9 +1,10 @@
 """Generate the golden fixtures in tests/golden/ from the reference itself.
 
-Run in a container that has the reference checkout at /root/reference and
-numba installed:
+Run in a container that has the reference checkout and numba installed,
+naming the checkout with ``--reference DIR`` or the ``TOD_REFERENCE_DIR``
+environment variable (default: /root/reference):
 
-    python tests/golden/make_golden.py
+    python tests/golden/make_golden.py --reference /path/to/checkout
 
 The reference's Numba kernels write their JIT cache next to their sources, so
 the script copies the checkout to /tmp/refcopy and points NUMBA_CACHE_DIR at
@@ -23,7 +24,7 @@ import shutil
 import sys
 import types
 
-REF = "/root/reference"
+REF = os.environ.get("TOD_REFERENCE_DIR", "/root/reference")
 COPY = "/tmp/refcopy"
 HERE = os.path.dirname(os.path.abspath(__file__))
 
@@ -337,6 +338,9 @@ def clusters_case():
 
 
 def main():
+    global REF
+    if "--reference" in sys.argv:
+        REF = sys.argv[sys.argv.index("--reference") + 1]
     if "--only-clusters" in sys.argv:
         np.savez_compressed(os.path.join(HERE, "clusters.npz"), **clusters_case())
         return

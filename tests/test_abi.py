@@ -118,3 +118,15 @@ def test_pointing_params_validation():
     assert lib.todgpu_pointing_params(*args(4, _native.F64, None)) == _native.EINVAL
     assert lib.todgpu_pointing_params(*args(0, _native.F32, None)) == 0
     assert lib.todgpu_last_error_string()
+
+
+def test_static_entry_rejects_nside_above_its_table():
+    """todgpu_gather_accum_static holds a ring table for nside <= 4096 only and
+    rejects larger maps before any CUDA call."""
+    lib = _native.lib()
+    a = _args(nside=8192, B=4, S=4, C=1, c_q=-1, c_u=-1, map_dtype=_native.F64, map_stride=12 * 8192 * 8192,
+              tod_stride=4)
+    for name in ("vec_orig", "axes", "cos_a", "sin_a", "ax_pts", "cos_p", "sin_p", "beam_vals", "map", "tod"):
+        setattr(a, name, 16)  # never dereferenced: the size check comes first
+    assert lib.todgpu_gather_accum_static(ctypes.byref(a), None) == _native.ENSIDE
+    assert b"4096" in lib.todgpu_last_error_string()

@@ -4,10 +4,12 @@ Some callers cannot allocate device memory -- for example a host application
 whose device memory is owned by another framework's allocator, or a foreign-
 language binding that can pass existing buffers but cannot create new ones.
 For them the library offers an entry point whose only scratch memory (the
-ring table) is a fixed-size array built into the library.  This test calls
-it through the C ABI twice in a row and checks both results against the
-regular entry point, which uses a caller-allocated ring table.  It is kept in
-a file of its own that pytest collects last.
+ring table) is a fixed-size array built into the library.  These tests call
+it through the C ABI twice in a row and check both results against the
+regular entry point, which uses a caller-allocated ring table, for every
+pointing mode (reference float32 parameters, float64 parameters, angles), a
+packed map and an entry without Q and U.  They are kept in a file of their
+own that pytest collects last.
 """
 
 import ctypes
@@ -17,8 +19,8 @@ import pytest
 import torch
 
 from tod_generation_mapbased_beam_b200 import _native
-from tod_generation_mapbased_beam_b200.kernels import (beam_reach, boresight_phi_host, make_args,
-                                                       ring_table)
+from tod_generation_mapbased_beam_b200.kernels import (beam_reach, boresight_phi_host, make_args, pack_map,
+                                                       pointing_params, ring_table)
 
 pytestmark = pytest.mark.gpu
 
@@ -41,34 +43,76 @@ def _inputs(nside, B, S, seed):
     mp = rng.standard_normal((3, 12 * nside * nside))
     bv = rng.uniform(0.1, 1.0, S).astype(np.float32)
     bv /= bv.sum()
-    return params, mp, bv
+    angles = (th, ph, psi.astype(np.float64))
+    return params, mp, bv, angles
 
 
-def _run(entry, interp, nside, params, mp, bv, table=None):
+def _args(pmode, interp, nside, params, angles, mp, bv, tod, comps, table):
+    """todgpu_gather_args for one pointing mode ("f32", "f64" or "angles")."""
     dev = torch.device("cuda")
     B, S = params[1].shape[0], params[0].shape[0]
-    tp = [torch.from_numpy(np.ascontiguousarray(p)).to(dev) for p in params]
-    bore = torch.from_numpy(boresight_phi_host(params[4])).to(dev)
+    C, c_q, c_u = (3, 1, 2) if comps == "IQU" else (1, -1, -1)
     beam = torch.from_numpy(bv).to(dev)
-    sky = torch.from_numpy(mp).to(dev)
-    tod = torch.zeros((3, B), dtype=torch.float64, device=dev)
-    args = make_args(interp, nside, B, S, 3, 1, 2, tp, np.float32, bore, beam, sky, tod, table=table)
+    if pmode == "f32":
+        tp = [torch.from_numpy(np.ascontiguousarray(p)).to(dev) for p in params]
+        bore = torch.from_numpy(boresight_phi_host(params[4])).to(dev)
+        a = make_args(interp, nside, B, S, C, c_q, c_u, tp, np.float32, bore, beam, mp, tod, table=table)
+        keep = tp + [bore]
+    else:
+        vec = torch.from_numpy(params[0].astype(np.float64)).to(dev)
+        th, ph, ps = (torch.from_numpy(x).to(dev) for x in angles)
+        if pmode == "f64":
+            rot = list(pointing_params(th, ph, ps, 0.3, 0.02))
+            a = make_args(interp, nside, B, S, C, c_q, c_u, [vec] + rot, np.float64, None, beam, mp, tod,
+                          table=table)
+            keep = [vec] + rot
+        else:
+            a = make_args(interp, nside, B, S, C, c_q, c_u, [vec] + [None] * 6, np.float64, None, beam, mp, tod,
+                          table=table)
+            a.params_dtype = _native.ANGLES
+            a.theta, a.phi, a.psi = th.data_ptr(), ph.data_ptr(), ps.data_ptr()
+            a.angles_dtype = _native.F64
+            a.center_phi, a.center_theta = 0.3, 0.02
+            keep = [vec, th, ph, ps]
+    return a, keep + [beam]
+
+
+def _run(entry, pmode, interp, nside, params, angles, mp, bv, comps="IQU", table=None):
+    dev = torch.device("cuda")
+    B = params[1].shape[0]
+    C = 3 if comps == "IQU" else 1
+    tod = torch.zeros((C, B), dtype=torch.float64, device=dev)
+    args, _keep = _args(pmode, interp, nside, params, angles, mp, bv, tod, comps, table)
     rc = entry(ctypes.byref(args), torch.cuda.current_stream().cuda_stream)
     _native.check(rc)
     torch.cuda.synchronize()
     return tod.cpu().numpy()
 
 
+def _map(mp, kind, comps):
+    sky = torch.from_numpy(mp if comps == "IQU" else mp[:1].copy()).cuda()
+    return sky if kind == "planar_f64" else pack_map(sky, kind)
+
+
 @pytest.mark.parametrize("interp", [_native.BILINEAR, _native.NEAREST])
-def test_static_entry_matches_regular_entry(interp):
+@pytest.mark.parametrize("pmode, kind, comps", [
+    ("f32", "planar_f64", "IQU"),
+    ("f64", "planar_f64", "IQU"),
+    ("angles", "planar_f64", "IQU"),
+    ("angles", "f32", "IQU"),
+    ("f32", "planar_f64", "I"),
+])
+def test_static_entry_matches_regular_entry(interp, pmode, kind, comps):
     lib = _native.lib()
     nside, B, S = 1024, 600, 800
-    params, mp, bv = _inputs(nside, B, S, seed=91)
+    params, mp, bv, angles = _inputs(nside, B, S, seed=91)
+    dmap = _map(mp, kind, comps)
     table = ring_table(nside, beam_reach(params[0], nside))
-    ref = _run(lib.todgpu_gather_accum, interp, nside, params, mp, bv, table=table)
-    first = _run(lib.todgpu_gather_accum_static, interp, nside, params, mp, bv)
-    second = _run(lib.todgpu_gather_accum_static, interp, nside, params, mp, bv)
+    ref = _run(lib.todgpu_gather_accum, pmode, interp, nside, params, angles, dmap, bv, comps, table=table)
+    first = _run(lib.todgpu_gather_accum_static, pmode, interp, nside, params, angles, dmap, bv, comps)
+    second = _run(lib.todgpu_gather_accum_static, pmode, interp, nside, params, angles, dmap, bv, comps)
     scale = np.abs(ref).max()
+    assert scale > 0
     assert np.abs(first - ref).max() <= TOD_RTOL * scale
     assert np.abs(second - ref).max() <= TOD_RTOL * scale
 
@@ -78,27 +122,9 @@ def test_static_entry_follows_a_different_nside():
     beam right after the first still matches the regular entry point."""
     lib = _native.lib()
     for nside, S, seed in ((256, 300, 5), (64, 120, 6)):
-        params, mp, bv = _inputs(nside, 200, S, seed)
+        params, mp, bv, angles = _inputs(nside, 200, S, seed)
+        dmap = _map(mp, "planar_f64", "IQU")
         table = ring_table(nside, beam_reach(params[0], nside))
-        ref = _run(lib.todgpu_gather_accum, _native.BILINEAR, nside, params, mp, bv, table=table)
-        got = _run(lib.todgpu_gather_accum_static, _native.BILINEAR, nside, params, mp, bv)
+        ref = _run(lib.todgpu_gather_accum, "f32", _native.BILINEAR, nside, params, angles, dmap, bv, table=table)
+        got = _run(lib.todgpu_gather_accum_static, "f32", _native.BILINEAR, nside, params, angles, dmap, bv)
         assert np.abs(got - ref).max() <= TOD_RTOL * np.abs(ref).max()
-
-
-def test_static_entry_rejects_nside_above_its_table():
-    lib = _native.lib()
-    a = _native.GatherArgs()
-    a.abi_version = _native.ABI_VERSION
-    a.interp = _native.BILINEAR
-    a.nside = 8192
-    a.B = 4
-    a.S = 4
-    a.C = 1
-    a.c_q = -1
-    a.c_u = -1
-    a.map_stride = 12 * 8192 * 8192
-    a.tod_stride = 4
-    for name in ("vec_orig", "axes", "cos_a", "sin_a", "ax_pts", "cos_p", "sin_p", "beam_vals", "map", "tod"):
-        setattr(a, name, 16)  # never dereferenced: the size check comes first
-    assert lib.todgpu_gather_accum_static(ctypes.byref(a), None) == _native.ENSIDE
-    assert b"4096" in lib.todgpu_last_error_string()

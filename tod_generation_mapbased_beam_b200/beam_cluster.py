@@ -26,6 +26,7 @@ candidates tie to the last bit.
 from __future__ import annotations
 
 import ctypes
+import logging
 import time
 
 import numpy as np
@@ -35,6 +36,15 @@ from . import _native
 from ._device import require_cuda, stream_handle
 
 __all__ = ["cluster_beam_pixels", "split_main_tail"]
+
+log = logging.getLogger(__name__)
+
+
+def _note(verbose, msg, *args):
+    """Progress report of the clustering, on this module's logger (INFO)
+    when ``verbose``."""
+    if verbose:
+        log.info(msg, *args)
 
 
 def split_main_tail(beam_vals, tail_fraction):
@@ -122,14 +132,12 @@ def _kmeans_sphere(vec, bvals, K, max_iter, tol, rng, label="", verbose=True):
         cos_disp = np.clip((centroids * new_centroids).sum(axis=1), -1.0, 1.0)
         centroids = new_centroids
         if cos_disp.min() > cos_tol:
-            if verbose:
-                print(f"    [cluster{label}] Converged at iter {iteration + 1}  "
-                      f"(max_disp={np.degrees(float(np.arccos(cos_disp).max())) * 60:.3f}')")
+            _note(verbose, "k-means%s: settled after %d iterations (largest centroid move %.3f arcmin)",
+                  label, iteration + 1, np.degrees(float(np.arccos(cos_disp).max())) * 60)
             break
     else:
-        if verbose:
-            print(f"    [cluster{label}] max_iter={max_iter} reached  "
-                  f"(max_disp={np.degrees(float(np.arccos(cos_disp).max())) * 60:.3f}')")
+        _note(verbose, "k-means%s: stopped at the iteration limit %d (largest centroid move %.3f arcmin)",
+              label, max_iter, np.degrees(float(np.arccos(cos_disp).max())) * 60)
     km.assign(centroids)
     return centroids, km.labels.cpu().numpy().astype(np.int32)
 
@@ -139,8 +147,8 @@ def _spread(vec, centroids, labels, label, verbose):
         return
     c = np.clip((vec * centroids[labels]).sum(axis=1), -1.0, 1.0)
     arcmin = np.degrees(np.arccos(c)) * 60.0
-    print(f"    [cluster{label}] Intra-cluster spread — mean={arcmin.mean():.2f}'  max={arcmin.max():.2f}'  "
-          f"95th={np.percentile(arcmin, 95):.2f}'")
+    _note(True, "k-means%s: pixel to centroid distance %.2f arcmin on average, %.2f at the 95th percentile, "
+          "%.2f at most", label, arcmin.mean(), np.percentile(arcmin, 95), arcmin.max())
 
 
 def cluster_beam_pixels(vec_orig, beam_vals, n_clusters, tail_fraction=None, max_iter=150, tol=1e-5,
@@ -162,9 +170,7 @@ def cluster_beam_pixels(vec_orig, beam_vals, n_clusters, tail_fraction=None, max
         weights = np.zeros(K, dtype=np.float64)
         np.add.at(weights, labels, bvals)
         weights /= weights.sum()
-        if verbose:
-            print(f"    [cluster] Full mode: {S} → {K} pixels  ({S / K:.1f}× reduction)  in "
-                  f"{time.time() - t0:.2f}s")
+        _note(verbose, "clustered all %d beam pixels into %d entries in %.2f s", S, K, time.time() - t0)
         _spread(vec, centroids, labels, "", verbose)
         return centroids.astype(np.float32), weights.astype(np.float32), labels
 
@@ -173,17 +179,16 @@ def cluster_beam_pixels(vec_orig, beam_vals, n_clusters, tail_fraction=None, max
     t0 = time.time()
     main_idx, tail_idx = split_main_tail(beam_vals, tail_fraction)
     n_main, n_tail = len(main_idx), len(tail_idx)
-    if verbose:
-        tp = float(beam_vals[tail_idx].sum())
-        print(f"    [cluster] Hybrid mode: {S} pixels  →  {n_main} main (top {100 * (1 - tp):.1f}% power, "
-              f"kept exact)  +  tail {n_tail} px ({100 * tp:.1f}% power, to be clustered)")
+    tp = float(beam_vals[tail_idx].sum())
+    _note(verbose, "main lobe: %d pixels kept as they are (%.1f%% of the weight); tail: %d pixels (%.1f%%)",
+          n_main, 100 * (1 - tp), n_tail, 100 * tp)
     K_tail = min(n_clusters, n_tail)
     if K_tail >= n_tail:
         vec_tail = vec_orig[tail_idx]
         bv_tail = beam_vals[tail_idx]
         tail_labels = np.arange(n_tail, dtype=np.int32)
-        if verbose:
-            print(f"    [cluster] Tail has only {n_tail} pixels — kept as-is (K_tail={K_tail})")
+        _note(verbose, "tail left unclustered: %d pixels, no more than the %d entries asked for", n_tail,
+              n_clusters)
     else:
         vec_t = vec_orig[tail_idx].astype(np.float64)
         bv_t = beam_vals[tail_idx].astype(np.float64)
@@ -194,9 +199,7 @@ def cluster_beam_pixels(vec_orig, beam_vals, n_clusters, tail_fraction=None, max
         np.add.at(cw, tail_labels, bv_t)
         vec_tail = centroids_t.astype(np.float32)
         bv_tail = cw.astype(np.float32)
-        if verbose:
-            print(f"    [cluster] Tail: {n_tail} → {K_tail} clusters  ({n_tail / K_tail:.1f}× reduction)  in "
-                  f"{time.time() - t0:.2f}s")
+        _note(verbose, "tail: %d pixels clustered into %d entries in %.2f s", n_tail, K_tail, time.time() - t0)
         _spread(vec_t, centroids_t, tail_labels, " tail", verbose)
     vec_out = np.concatenate([vec_orig[main_idx], vec_tail], axis=0)
     bv_out = np.concatenate([beam_vals[main_idx], bv_tail], axis=0)
@@ -204,7 +207,5 @@ def cluster_beam_pixels(vec_orig, beam_vals, n_clusters, tail_fraction=None, max
     labels = np.empty(S, dtype=np.int32)
     labels[main_idx] = np.arange(n_main, dtype=np.int32)
     labels[tail_idx] = n_main + tail_labels
-    if verbose:
-        print(f"    [cluster] Combined: {S} → {n_main + K_tail} pixels  ({S / (n_main + K_tail):.1f}× total "
-              f"reduction)")
+    _note(verbose, "beam entry now has %d pixels in place of %d", n_main + K_tail, S)
     return vec_out, bv_out, labels

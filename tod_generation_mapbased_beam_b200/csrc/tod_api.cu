@@ -491,22 +491,28 @@ extern "C" int todgpu_gather_accum_static(const todgpu_gather_args* a, void* str
   if (rc != TODGPU_OK) return rc;
   KArgs k = make_kargs(a);
   cudaStream_t s = static_cast<cudaStream_t>(stream);
+  const bool has_qu = (a->c_q >= 0 && a->c_u >= 0);
   if (!(a->flags & TODGPU_FLAG_NO_TABLES)) {
     // every call rebuilds the whole table (header, records, prefix sums) for
-    // its own nside and beam, so nothing depends on earlier contents
-    if (a->params_dtype == TODGPU_F32)
-      static_reach_kernel<kParamsRef32><<<1, kNTStatic, 0, s>>>(k, t);
-    else
-      static_reach_kernel<kParamsF64><<<1, kNTStatic, 0, s>>>(k, t);
-    ring_table_kernel<<<grid_for(4 * a->nside, 256), 256, 0, s>>>(a->nside, 0.0, t, true);
-    ring_prefix_kernel<<<1, 1024, 0, s>>>(a->nside, t);
+    // its own nside and beam, so nothing depends on earlier contents.  Without
+    // Q and U the gather reads only the ring records (no spin-2 tables): the
+    // header then carries a zero reach and the slot sums are not built.
+    if (has_qu) {
+      if (a->params_dtype == TODGPU_F32)
+        static_reach_kernel<kParamsRef32><<<1, kNTStatic, 0, s>>>(k, t);
+      else
+        static_reach_kernel<kParamsF64><<<1, kNTStatic, 0, s>>>(k, t);
+      ring_table_kernel<<<grid_for(4 * a->nside, 256), 256, 0, s>>>(a->nside, 0.0, t, true);
+      ring_prefix_kernel<<<1, 1024, 0, s>>>(a->nside, t);
+    } else {
+      ring_table_kernel<<<grid_for(4 * a->nside, 256), 256, 0, s>>>(a->nside, 0.0, t, false);
+    }
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return cuda_fail(e, "built-in ring table kernels");
     k.ring_table = t;
   } else {
     k.ring_table = nullptr;
   }
-  const bool has_qu = (a->c_q >= 0 && a->c_u >= 0);
   return dispatch_types(k, a->interp, has_qu, a->map_dtype, a->params_dtype, s);
 }
 

@@ -148,7 +148,9 @@ class LearnedTailTOD:
     def judge(self, theta, phi, psi, budget_uK=0.1):
         """Errors in uK of the learned form against the plain float64 method on
         the given (held-out) samples, and of the same form with the tail
-        dropped.  Sets the fallback decision for ``tod(tail="auto")``."""
+        dropped.  Sets the fallback decision for ``tod(tail="auto")``: the
+        network is used only if the RMS error of every Stokes component is
+        within ``budget_uK``."""
         ref = self.full_plain(theta, phi, psi)
         main = self.main_lobe(theta, phi, psi)
         learned = self.learned_tail(theta, phi, psi, main.clone())
@@ -162,7 +164,7 @@ class LearnedTailTOD:
         out = dict(samples=int(ref.shape[1]), learned=stats(learned - ref), dropped=stats(main - ref),
                    tail_rms_uK=(tail.std(dim=1).cpu().numpy() * 1e6).tolist(),
                    surrogate=stats(learned - main - tail), budget_uK=float(budget_uK))
-        out["use_surrogate"] = out["learned"]["rms_all_uK"] <= budget_uK
+        out["use_surrogate"] = max(out["learned"]["rms_uK"]) <= budget_uK
         self.judged = out
         return out
 

@@ -12,7 +12,10 @@ accumulator (tod_core.py:128) and the float32 cast of the result
 
 Differences, all additive:
 * map, beam vectors and weights may be torch CUDA tensors (zero copy); numpy
-  inputs are uploaded once per array object and cached on the device;
+  inputs are uploaded once per array object and cached on the device, and
+  re-uploaded when their contents change (every call checks a CRC-32 of the
+  host bytes, so a buffer refilled in place is read again, as the reference
+  reads its inputs on every call);
 * without ``data["mp_stacked"]`` the ``mp`` component list is stacked and
   uploaded (the reference falls back to a healpy path there, which needs
   healpy; the result is the same gather);
@@ -30,6 +33,7 @@ from __future__ import annotations
 
 import os
 import weakref
+import zlib
 
 import numpy as np
 import torch
@@ -43,9 +47,35 @@ from .tod_rotations import _rotation_params, precompute_rotation_vector_batch  #
 _INTERP = {"bilinear": _native.BILINEAR, "nearest": _native.NEAREST}
 
 
+# Host arrays of a few MiB or more are fingerprinted in chunks of this many
+# bytes on the preparation thread pool.
+_FP_CHUNK = 1 << 23
+
+
+def _fingerprint(arr):
+    """CRC-32 of every byte of a host array (chunk by chunk, in parallel for
+    large arrays; zlib releases the GIL).  Position-sensitive, so a refill of
+    the same buffer with other or permuted values changes it."""
+    a = np.ascontiguousarray(arr)
+    mv = memoryview(a.reshape(-1)).cast("B")
+    n = mv.nbytes
+    if n <= _FP_CHUNK:
+        return (a.dtype.str, a.shape, zlib.crc32(mv))
+    bounds = [(i, min(n, i + _FP_CHUNK)) for i in range(0, n, _FP_CHUNK)]
+    crcs = tuple(_pool().map(lambda b: zlib.crc32(mv[b[0]:b[1]]), bounds))
+    return (a.dtype.str, a.shape, crcs)
+
+
 class _UploadCache:
-    """Device copies of read-only host arrays, keyed by array identity and
-    dropped when the host array is garbage-collected."""
+    """Device copies of host arrays, keyed by array identity and dropped when
+    the host array is garbage-collected.  Every call checks the host array's
+    content (CRC-32 of all its bytes, see :func:`_fingerprint`) and uploads it
+    again if it changed: the reference reads its inputs on every call
+    (tod_core.py:121-160), so a caller that refills the same buffer in place
+    gets the new values.  ``CHECK_CONTENT = False`` trusts identity alone
+    (for callers that never modify an array they have passed)."""
+
+    CHECK_CONTENT = True
 
     def __init__(self):
         self._store = {}
@@ -56,57 +86,74 @@ class _UploadCache:
             return t.contiguous()
         key = (id(arr), np.dtype(dtype).str if not isinstance(dtype, torch.dtype) else str(dtype))
         hit = self._store.get(key)
+        fp = None
         if hit is not None and hit[1]() is arr:
-            return hit[0]
+            if not self.CHECK_CONTENT:
+                return hit[0]
+            fp = _fingerprint(arr)
+            if fp == hit[2]:
+                return hit[0]
         np_dt = {torch.float32: np.float32, torch.float64: np.float64}[dtype]
         t = torch.from_numpy(np.ascontiguousarray(arr, dtype=np_dt)).to("cuda")
+        if fp is None:
+            fp = _fingerprint(arr) if self.CHECK_CONTENT else None
         try:
             ref = weakref.ref(arr, lambda _r, k=key: self._store.pop(k, None))
         except TypeError:
             return t
-        self._store[key] = (t, ref)
+        self._store[key] = (t, ref, fp)
         return t
 
 
 _cache = _UploadCache()
 
 
-class _BeamCache:
-    """Device copies of beams (pixel vectors, weights) with the pixels in
-    ``kernels.beam_order`` -- the layout the gather reads fastest, like the
-    float64 map records -- keyed by the identity of both host arrays and
-    dropped with them.  Only the order of the sum over pixels differs from the
-    given order (float64 results within a few ulps)."""
+def _tensor_key(t):
+    """Identity of a device tensor's current contents: the object and its
+    in-place modification counter."""
+    return (id(t), t._version)
+
+
+class _DerivedCache:
+    """Device arrays derived from device tensors (a beam in gather order, a
+    stacked or packed map), keyed by the sources' identity and modification
+    counters and dropped with them."""
 
     def __init__(self):
         self._store = {}
 
-    def get(self, vec_orig, beam_vals, vec_dtype):
-        key = (id(vec_orig), id(beam_vals), str(vec_dtype))
+    def get(self, sources, extra, make):
+        key = tuple(_tensor_key(t) for t in sources) + (extra,)
         hit = self._store.get(key)
-        if hit is not None and hit[2]() is vec_orig and hit[3]() is beam_vals:
-            return hit[0], hit[1]
-        idx = torch.from_numpy(beam_order(vec_orig))
-        vec = _cache.get(vec_orig, vec_dtype).reshape(-1, 3)
-        bv = _cache.get(beam_vals, torch.float32).reshape(-1)
-        dev = vec.device
-        vec = vec[idx.to(dev)].contiguous()
-        bv = bv[idx.to(dev)].contiguous()
+        if hit is not None and all(r() is t for r, t in zip(hit[1], sources)):
+            return hit[0]
+        val = make()
         try:
             drop = lambda _r, k=key: self._store.pop(k, None)  # noqa: E731
-            self._store[key] = (vec, bv, weakref.ref(vec_orig, drop), weakref.ref(beam_vals, drop))
+            self._store[key] = (val, [weakref.ref(t, drop) for t in sources])
         except TypeError:
             pass
-        return vec, bv
+        return val
 
 
-_beams = _BeamCache()
+_derived = _DerivedCache()
 
 
 def device_beam(vec_orig, beam_vals, vec_dtype=torch.float64):
-    """(vec (S, 3), beam_vals (S,)) of a beam on the device, pixels in the
-    gather's preferred order (cached per pair of host arrays)."""
-    return _beams.get(vec_orig, beam_vals, vec_dtype)
+    """(vec (S, 3), beam_vals (S,)) of a beam on the device with the pixels in
+    ``kernels.beam_order`` -- the layout the gather reads fastest, like the
+    float64 map records (cached per pair of inputs while their contents are
+    unchanged).  Only the order of the sum over pixels differs from the given
+    order (float64 results within a few ulps)."""
+    vec = _cache.get(vec_orig, vec_dtype)
+    bv = _cache.get(beam_vals, torch.float32)
+
+    def make():
+        v = vec.reshape(-1, 3)
+        idx = torch.from_numpy(beam_order(v)).to(v.device)
+        return v[idx].contiguous(), bv.reshape(-1)[idx].contiguous()
+
+    return _derived.get((vec, bv), ("beam", str(vec_dtype)), make)
 
 
 def _map_dtype(mp):
@@ -121,43 +168,22 @@ def stacked_map(data, mp):
     ms = data.get("mp_stacked")
     if ms is not None:
         return _cache.get(ms, _map_dtype(ms))
-    comps = data["comp_indices"]
-    key = "_todgpu_stacked"
-    cached = data.get(key)
-    if cached is not None:
-        return cached
-    parts = [mp[c] for c in comps]
-    if all(is_tensor(p) for p in parts):
-        t = torch.stack([p.to("cuda") for p in parts]).contiguous()
-    else:
-        arr = np.stack([np.asarray(p) for p in parts])
-        t = torch.from_numpy(arr).to("cuda").contiguous()
-    data[key] = t
-    return t
-
-
-_packed = {}  # id(planar device map) -> (PackedMap, weak reference to the planar map)
+    parts = [mp[c] for c in data["comp_indices"]]
+    dt = torch.float64 if any(_map_dtype(p) == torch.float64 for p in parts) else torch.float32
+    devs = [_cache.get(p, dt) for p in parts]
+    return _derived.get(devs, "stack", lambda: torch.stack([d.reshape(-1) for d in devs]).contiguous())
 
 
 def device_map(data, mp):
     """The entry's device map in the layout the kernels read fastest: a
     float64 map of up to 4 components as float64 records {I, Q, U, 0}
-    (packed once and cached; the TOD is the same bit for bit), a float32 map
-    planar (its float32 products are part of the reference's result)."""
+    (packed once and cached while its contents are unchanged; the TOD is the
+    same bit for bit), a float32 map planar (its float32 products are part of
+    the reference's result)."""
     t = stacked_map(data, mp)
     if t.dtype != torch.float64 or t.shape[0] > 4:
         return t
-    key = id(t)
-    hit = _packed.get(key)
-    if hit is not None and hit[1]() is t:
-        return hit[0]
-    pm = pack_map(t, "f64")
-    try:
-        ref = weakref.ref(t, lambda _r, k=key: _packed.pop(k, None))
-    except TypeError:
-        return pm
-    _packed[key] = (pm, ref)
-    return pm
+    return _derived.get((t,), "f64_records", lambda: pack_map(t, "f64"))
 
 
 def component_slots(comp_indices):

@@ -88,6 +88,8 @@ def parse_args():
     p.add_argument("--learned-steps", type=int, default=4000, help="training steps of the learned tail")
     p.add_argument("--no-tables", action="store_true",
                    help="evaluate ring data and spin-2 angles directly (A/B comparison)")
+    p.add_argument("--no-beam-stage", action="store_true",
+                   help="read the beam from global memory instead of shared memory (A/B comparison)")
     p.add_argument("--cpu-seconds", type=float, default=10.0,
                    help="target CPU time of the bounded CPU-baseline sample")
     return p.parse_args()
@@ -97,8 +99,8 @@ def g4(x):
     """x rounded to 4 significant digits (keeps the JSON line short)."""
     if x is None:
         return None
-    if isinstance(x, (list, tuple)):
-        return [g4(v) for v in x]
+    if isinstance(x, (list, tuple, np.ndarray)):
+        return [g4(v) for v in np.asarray(x).reshape(-1)]
     return float(f"{float(x):.4g}")
 
 
@@ -448,8 +450,9 @@ def run_ours(args, dist):
     modes = [args.mode] + ([] if args.no_other_mode else [m for m in STENCIL if m != args.mode])
     interp = {"bilinear": _native.BILINEAR, "nearest": _native.NEAREST}
     tods = {m: torch.zeros((3, B), dtype=torch.float64, device=dev) for m in modes}
+    flags = _native.FLAG_NO_BEAM_STAGE if args.no_beam_stage else 0
     cargs = {m: make_args(interp[m], nside, B, S, 3, 1, 2, params, np.float32, bore, bv, sky_rec, tods[m],
-                          table=table) for m in modes}
+                          table=table, flags=flags) for m in modes}
 
     def launch(m):
         _native.check(lib.todgpu_gather_accum(ctypes.byref(cargs[m]), stream.cuda_stream))
@@ -561,7 +564,7 @@ def run_ours(args, dist):
         for kind in ("planar_f64", "f32", "bf16"):
             pm = sky if kind == "planar_f64" else pack_map(sky, kind)
             margs = make_args(interp[args.mode], nside, B, S, 3, 1, 2, params, np.float32, bore, bv, pm, tod,
-                              table=table)
+                              table=table, flags=flags)
             for _ in range(2):
                 _native.check(lib.todgpu_gather_accum(ctypes.byref(margs), stream.cuda_stream))
             torch.cuda.synchronize()
@@ -663,7 +666,8 @@ def run_precision(args, dist, sky):
 
         def launch():
             tod.zero_()
-            gather_accum_angles(interp, vec, *ang, 0.0, 0.0, 2048, mp, bv, tod, c_q=1, c_u=2)
+            gather_accum_angles(interp, vec, *ang, 0.0, 0.0, 2048, mp, bv, tod, c_q=1, c_u=2,
+                                flags=_native.FLAG_NO_BEAM_STAGE if args.no_beam_stage else 0)
 
         launch()
         ms = dist.max(_evt_ms(launch, stream))

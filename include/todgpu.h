@@ -38,6 +38,8 @@ extern "C" {
 /* Flags (todgpu_gather_args.flags). */
 #define TODGPU_FLAG_NO_TABLES 1 /* ignore ring_table: evaluate every stencil ring and spin-2
                                    angle directly (same results, slower) */
+#define TODGPU_FLAG_NO_BEAM_STAGE 2 /* read the beam from global memory even when the launch
+                                       could hold it in shared memory (same results) */
 
 /* Element types. */
 #define TODGPU_F32 0
@@ -129,8 +131,19 @@ typedef struct todgpu_gather_args {
 
 /* Fused rotate -> HEALPix stencil -> spin-2 -> gather -> accumulate.
  * Replaces tod_bilinear._gather_accum_fused_jit (tod_bilinear.py:205-477)
- * and tod_nearest._gather_accum_nearest_jit (tod_nearest.py:21-158). */
+ * and tod_nearest._gather_accum_nearest_jit (tod_nearest.py:21-158).
+ * vec_orig must be aligned to its element size and beam_vals to 4 bytes;
+ * S is at most 2^29.  When the beam fits in shared memory beside the spin-2
+ * table, every CTA copies it there once per launch with bulk copies. */
 int todgpu_gather_accum(const todgpu_gather_args *args, void *stream);
+
+/* Number of bounded waits of the gather kernels (the beam's bulk copies into
+ * shared memory) that ran out since the library was loaded: 0 in a healthy
+ * run.  A CTA whose wait ran out copies the beam with plain loads instead,
+ * so its results stay correct; the call's err_count, when given, counts it
+ * too.  Reading it synchronises the device; -1 on a CUDA error.  No
+ * counterpart in the reference. */
+int64_t todgpu_gather_wait_timeouts(void);
 
 /* Many jobs in one persistent launch: jobs[0 .. njobs) (a host array) are
  * independent gathers -- typically one detector each, with its own beam

@@ -21,6 +21,7 @@ BILINEAR, NEAREST = 0, 1
 F32, F64, ANGLES = 0, 1, 2
 PACKED_F32, PACKED_BF16, PACKED_F64 = 2, 3, 4
 FLAG_NO_TABLES = 1
+FLAG_NO_BEAM_STAGE = 2
 
 _i32 = ctypes.c_int32
 _i64 = ctypes.c_int64
@@ -110,6 +111,8 @@ def _declare(lib):
     lib.todgpu_gather_accum_batched.restype = ctypes.c_int
     lib.todgpu_gather_accum_static.argtypes = [ctypes.POINTER(GatherArgs), _p]
     lib.todgpu_gather_accum_static.restype = ctypes.c_int
+    lib.todgpu_gather_wait_timeouts.argtypes = []
+    lib.todgpu_gather_wait_timeouts.restype = _i64
     lib.todgpu_bilinear_stencils.argtypes = [ctypes.POINTER(GatherArgs), _p, _p, _p]
     lib.todgpu_bilinear_stencils.restype = ctypes.c_int
     lib.todgpu_get_interp_weights.argtypes = [_i64, _p, _p, _i64, _p, _p, _p]
@@ -218,6 +221,7 @@ def exported_symbols():
         "todgpu_gather_accum",
         "todgpu_gather_accum_batched",
         "todgpu_gather_accum_static",
+        "todgpu_gather_wait_timeouts",
         "todgpu_bilinear_stencils",
         "todgpu_get_interp_weights",
         "todgpu_ang2pix",

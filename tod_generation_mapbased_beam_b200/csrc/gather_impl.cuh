@@ -89,28 +89,27 @@ struct KArgs {
   double* tod;
   long long tod_stride;
   unsigned long long* err;
+  int flags_stage;           // the caller allows staging the beam in shared memory
+  int beam_stage;            // the launch made room for the beam in shared memory
 };
 
 // Pointing modes of the per-sample rotation.
 constexpr int kParamsRef32 = 0;  // reference float32 parameter arrays
 constexpr int kParamsF64 = 1;    // float64 parameter arrays
 constexpr int kAngles = 2;       // (theta, phi, psi) + beam centre, derived on the device
-constexpr int kParamsF64Shared = 3;  // float64 parameter arrays, loaded once per CTA (large beams)
 
-__host__ __device__ constexpr bool f64_params(int pm) { return pm == kParamsF64 || pm == kParamsF64Shared; }
+__host__ __device__ constexpr bool f64_params(int pm) { return pm == kParamsF64; }
 
 template <int PM>
 __device__ __forceinline__ double angle_at(const KArgs& a, const void* p, long long b) {
   return a.angles_f32 ? (double)static_cast<const float*>(p)[b] : static_cast<const double*>(p)[b];
 }
 
-// Rotation of sample b from its pointing angles, in float64: the Rodrigues
+// Rotation from pointing angles (theta, phi, psi), in float64: the Rodrigues
 // vector taking the beam centre c to the boresight t and the polarisation
 // offset beta (tod_rotations.py:219-303), then the parameters of
 // tod_rotations.py:306-333 without any float32 rounding.
-__device__ __forceinline__ SampleRot rot_from_angles(const KArgs& a, long long b) {
-  const double th = angle_at<kAngles>(a, a.theta, b), ph = angle_at<kAngles>(a, a.phi, b);
-  const double ps = angle_at<kAngles>(a, a.psi, b);
+__device__ __forceinline__ SampleRot rot_from_angle_values(const KArgs& a, double th, double ph, double ps) {
   double st, ct, sp, cp;
   sincos(th, &st, &ct);
   sincos(ph, &sp, &cp);
@@ -151,42 +150,77 @@ __device__ __forceinline__ SampleRot rot_from_angles(const KArgs& a, long long b
   return r;
 }
 
+__device__ __forceinline__ SampleRot rot_from_angles(const KArgs& a, long long b) {
+  return rot_from_angle_values(a, angle_at<kAngles>(a, a.theta, b), angle_at<kAngles>(a, a.phi, b),
+                               angle_at<kAngles>(a, a.psi, b));
+}
+
+// The per-sample pointing inputs as numbered fields.  Reference float32
+// parameters: 0-2 axes, 3 cos_a, 4 sin_a, 5-7 ax_pts, 8 cos_p, 9 sin_p, 10 the
+// boresight longitude (when given); float64 parameters: fields 0-9 as
+// doubles; angles: 0 theta, 1 phi, 2 psi.  field_ptr gives a field's address
+// (nullptr when absent), field_bytes its size.
 template <int PM>
-__device__ __forceinline__ SampleRot load_rot(const KArgs& a, long long b) {
+__device__ __forceinline__ const void* field_ptr(const KArgs& a, long long b, int i) {
+  if constexpr (PM == kAngles) {
+    const void* p = i == 0 ? a.theta : (i == 1 ? a.phi : a.psi);
+    return a.angles_f32 ? (const void*)(static_cast<const float*>(p) + b)
+                        : (const void*)(static_cast<const double*>(p) + b);
+  } else {
+    using T = typename std::conditional<PM == kParamsRef32, float, double>::type;
+    if (i < 3) return static_cast<const T*>(a.axes) + 3 * b + i;
+    if (i == 3) return static_cast<const T*>(a.cos_a) + b;
+    if (i == 4) return static_cast<const T*>(a.sin_a) + b;
+    if (i < 8) return static_cast<const T*>(a.pts) + 3 * b + (i - 5);
+    if (i == 8) return static_cast<const T*>(a.cos_p) + b;
+    if (i == 9) return static_cast<const T*>(a.sin_p) + b;
+    if (PM == kParamsRef32 && i == 10 && a.bore_phi != nullptr) return a.bore_phi + b;
+    return nullptr;
+  }
+}
+template <int PM>
+__device__ __forceinline__ int field_count() {
+  return PM == kAngles ? 3 : (PM == kParamsRef32 ? 11 : 10);
+}
+template <int PM>
+__device__ __forceinline__ int field_bytes(const KArgs& a) {
+  return PM == kParamsRef32 ? 4 : (PM == kAngles && a.angles_f32 ? 4 : 8);
+}
+
+// Rotation of a sample from its fields, got(i) returning field i (float for
+// the reference typing, double otherwise).
+template <int PM, class Get>
+__device__ __forceinline__ SampleRot rot_from_fields(const KArgs& a, const Get& got) {
   SampleRot r;
   if constexpr (PM == kAngles) {
-    r = rot_from_angles(a, b);
+    r = rot_from_angle_values(a, got(0), got(1), got(2));
   } else if constexpr (f64_params(PM)) {
-    const double* ax = static_cast<const double*>(a.axes) + 3 * b;
-    const double* pt = static_cast<const double*>(a.pts) + 3 * b;
-    r.kx = ax[0];
-    r.ky = ax[1];
-    r.kz = ax[2];
-    r.ca = static_cast<const double*>(a.cos_a)[b];
-    r.sa = static_cast<const double*>(a.sin_a)[b];
-    r.px = pt[0];
-    r.py = pt[1];
-    r.pz = pt[2];
-    r.cp = static_cast<const double*>(a.cos_p)[b];
-    r.sp = static_cast<const double*>(a.sin_p)[b];
+    r.kx = got(0);
+    r.ky = got(1);
+    r.kz = got(2);
+    r.ca = got(3);
+    r.sa = got(4);
+    r.px = got(5);
+    r.py = got(6);
+    r.pz = got(7);
+    r.cp = got(8);
+    r.sp = got(9);
   } else {
-    const float* ax = static_cast<const float*>(a.axes) + 3 * b;
-    const float* pt = static_cast<const float*>(a.pts) + 3 * b;
-    r.fkx = ax[0];
-    r.fky = ax[1];
-    r.fkz = ax[2];
-    r.fca = static_cast<const float*>(a.cos_a)[b];
-    r.fsa = static_cast<const float*>(a.sin_a)[b];
+    r.fkx = got(0);
+    r.fky = got(1);
+    r.fkz = got(2);
+    r.fca = got(3);
+    r.fsa = got(4);
     r.kx = (double)r.fkx;
     r.ky = (double)r.fky;
     r.kz = (double)r.fkz;
     r.ca = (double)r.fca;
     r.sa = (double)r.fsa;
-    r.px = (double)pt[0];
-    r.py = (double)pt[1];
-    r.pz = (double)pt[2];
-    r.cp = (double)static_cast<const float*>(a.cos_p)[b];
-    r.sp = (double)static_cast<const float*>(a.sin_p)[b];
+    r.px = (double)got(5);
+    r.py = (double)got(6);
+    r.pz = (double)got(7);
+    r.cp = (double)got(8);
+    r.sp = (double)got(9);
   }
   return r;
 }
@@ -194,44 +228,56 @@ __device__ __forceinline__ SampleRot load_rot(const KArgs& a, long long b) {
 // Boresight (z, sin theta, phi) of the spin-2 angle.  Float32 parameters use
 // the reference's typing: sin theta from a float32 square, phi from float32
 // atan2 (host libm value when provided).
-template <int PM>
-__device__ __forceinline__ void load_boresight(const KArgs& a, const SampleRot& rot, long long b, double& z,
-                                               double& sth, double& phi) {
+template <int PM, class Get>
+__device__ __forceinline__ void boresight_from_fields(const KArgs& a, const SampleRot& rot, const Get& got, double& z,
+                                                      double& sth, double& phi) {
   if constexpr (PM == kAngles) {
     z = clamp1(rot.pz);
     sth = sqrt(max0(1.0 - rot.pz * rot.pz));
     phi = atan2(rot.py, rot.px);
   } else if constexpr (f64_params(PM)) {
-    const double* pt = static_cast<const double*>(a.pts) + 3 * b;
-    z = clamp1(pt[2]);
-    sth = sqrt(max0(1.0 - pt[2] * pt[2]));
-    phi = atan2(pt[1], pt[0]);
+    const double pz = got(7);
+    z = clamp1(pz);
+    sth = sqrt(max0(1.0 - pz * pz));
+    phi = atan2((double)got(6), (double)got(5));
   } else {
-    const float* pt = static_cast<const float*>(a.pts) + 3 * b;
-    const float bz = pt[2];
+    const float bz = got(7);
     const float bz2 = bz * bz;
     z = clamp1((double)bz);
     sth = sqrt(max0(1.0 - (double)bz2));
     if (a.bore_phi != nullptr)
-      phi = (double)a.bore_phi[b];
+      phi = (double)got(10);
     else
-      phi = (double)(float)atan2((double)pt[1], (double)pt[0]);
+      phi = (double)(float)atan2((double)got(6), (double)got(5));
   }
   if (phi < 0.0) phi += kTwoPi;
 }
 
-// Rotated beam pixel s of the sample (float64 beam vectors in the float64
-// and angles modes).
+// Field getter reading global memory.
 template <int PM>
-__device__ __forceinline__ void rotate_pixel(const KArgs& a, const SampleRot& r, long long s, double& vx,
-                                             double& vy, double& vz) {
-  if constexpr (PM != kParamsRef32) {
-    const double* v = static_cast<const double*>(a.vec) + 3 * s;
-    rot_f64(r, __ldg(v), __ldg(v + 1), __ldg(v + 2), vx, vy, vz);
-  } else {
-    const float* v = static_cast<const float*>(a.vec) + 3 * s;
-    rot_ref32(r, __ldg(v), __ldg(v + 1), __ldg(v + 2), vx, vy, vz);
+struct GlobalFields {
+  const KArgs& a;
+  long long b;
+  __device__ __forceinline__ auto operator()(int i) const {
+    if constexpr (PM == kParamsRef32)
+      return *static_cast<const float*>(field_ptr<PM>(a, b, i));
+    else if constexpr (PM == kAngles)
+      return a.angles_f32 ? (double)*static_cast<const float*>(field_ptr<PM>(a, b, i))
+                          : *static_cast<const double*>(field_ptr<PM>(a, b, i));
+    else
+      return *static_cast<const double*>(field_ptr<PM>(a, b, i));
   }
+};
+
+template <int PM>
+__device__ __forceinline__ SampleRot load_rot(const KArgs& a, long long b) {
+  return rot_from_fields<PM>(a, GlobalFields<PM>{a, b});
+}
+
+template <int PM>
+__device__ __forceinline__ void load_boresight(const KArgs& a, const SampleRot& rot, long long b, double& z,
+                                               double& sth, double& phi) {
+  boresight_from_fields<PM>(a, rot, GlobalFields<PM>{a, b}, z, sth, phi);
 }
 
 struct PackF32;
@@ -357,21 +403,26 @@ __device__ __forceinline__ double warp_sum(double v) {
 // the per-sample spin-2 table (shared memory).
 // ---------------------------------------------------------------------------
 
-// One RING ring.  Record 0 is a header: z = nside, ta = reach [rad].
+// One RING ring.  Record 0 is a header: z = nside, ta = reach [rad].  The
+// fields come in 16-byte pairs in the order the stencil reads them: {z, sth},
+// {phi0, dphi}, {ta, inv_dta}, {first32, n, inv_dphi}.
 struct __align__(16) RingRec {
-  double z;      // ring centre z
-  double ta;     // acos(z)
-  double sth;    // sqrt(max(0, 1 - z^2))
-  double phi0;   // longitude of the first pixel
-  double dphi;   // pixel spacing
-  long long first;
-  int n;         // pixels in the ring
-  int cap;       // spin-2 table slots reserved for this ring
-  long long pre; // sum of cap over rings 1 .. ir-1
-  double inv_dphi;  // 1 / dphi, correctly rounded
+  double z;         // ring centre z
+  double sth;       // sqrt(max(0, 1 - z^2))
+  double phi0;      // longitude of the first pixel
+  double dphi;      // pixel spacing
+  double ta;        // acos(z)
   double inv_dta;   // 1 / (ta(ir + 1) - ta), correctly rounded (0 for the last ring)
+  int first32;      // first pixel index in 32 bits (exact while 12 nside^2 < 2^31)
+  int n;            // pixels in the ring
+  double inv_dphi;  // 1 / dphi, correctly rounded
+  long long first;  // first pixel index
+  int cap;          // spin-2 table slots reserved for this ring
+  int unused;
 };
 static_assert(sizeof(RingRec) == 80, "RingRec must be 80 bytes");
+static_assert(offsetof(RingRec, phi0) == 16 && offsetof(RingRec, ta) == 32 && offsetof(RingRec, first32) == 48,
+              "RingRec pairs must sit on 16-byte boundaries");
 
 // Ring provider backed by the global ring table.
 struct TableRings {
@@ -390,22 +441,191 @@ struct TableRings {
   __device__ __forceinline__ double sth(long long ir, const RingData&) const { return __ldg(&t[ir].sth); }
 };
 
-// Per-sample spin-2 table: for window ring r (ring ir_lo + r) the slots
-// [off[r], off[r] + cap_r) hold cos 2d / sin 2d of in-ring pixels
-// iplo[r], iplo[r] + 1, ... (mod n).
+// Per-sample spin-2 table: window ring r (ring ir_lo + r) has ring[r] =
+// {off, iplo, cap, 0}: slots [off, off + cap) hold cos 2d / sin 2d of its
+// in-ring pixels iplo, iplo + 1, ... (mod n).  hdr = {ir_lo in 32 bits, window
+// rings (0: no table for this sample), filled slots, 0}.
 struct Spin2Tab {
+  int4 hdr;
   long long ir_lo;
-  int ir_lo32;   // ir_lo as a 32-bit index (fast path)
-  int nr;        // window rings (0: no table for this sample)
-  int total;     // filled slots
-  int off[kRingCap];
-  int iplo[kRingCap];
-  int cap[kRingCap];
+  long long unused;
+  int4 ring[kRingCap];
 };
 
 struct Bore {
   double z, sth, phi;
 };
+
+// One sample's rotation and boresight in shared memory, written by one thread
+// and read by all: the roll about the boresight p (cos/sin psi and 1 - cos
+// psi), the recentring about axis k (float64 form with 1 - cos a; for float32
+// parameters the reference's float32 inputs, and 1 - (double) cos a), and the
+// boresight (z, sin theta, phi) of the spin-2 angle.  Pairs sit on 16-byte
+// boundaries for 16-byte shared loads.
+struct __align__(16) SampleBlock {
+  double px, py, pz, cp, sp, omp;
+  double kx, ky, kz, ca, sa, oma;
+  float fkx, fky, fkz, fca, fsa, fpad0, fpad1, fpad2;
+  double bz, bsth, bphi, bpad;
+};
+static_assert(sizeof(SampleBlock) == 160, "SampleBlock layout");
+
+// A sample's pointing fields in shared memory, brought there by cp.async one
+// sample ahead (field i at byte 4 i for the reference float32 parameters, at
+// byte 8 i otherwise).
+struct __align__(16) RawFields {
+  unsigned long long v[12];
+};
+
+template <int PM>
+struct SharedFields {
+  const KArgs& a;
+  const RawFields& raw;
+  __device__ __forceinline__ auto operator()(int i) const {
+    if constexpr (PM == kParamsRef32)
+      return reinterpret_cast<const float*>(raw.v)[i];
+    else if constexpr (PM == kAngles)
+      return a.angles_f32 ? (double)reinterpret_cast<const float*>(raw.v)[2 * i]
+                          : reinterpret_cast<const double*>(raw.v)[i];
+    else
+      return reinterpret_cast<const double*>(raw.v)[i];
+  }
+};
+
+// Lane `lane` of one warp starts the copy of field `lane` of sample b into raw
+// (cp.async, this GPU's memory); every lane commits its group.
+template <int PM>
+__device__ __forceinline__ void prefetch_fields(const KArgs& a, long long b, RawFields& raw, int lane) {
+  if (lane < field_count<PM>()) {
+    const void* src = field_ptr<PM>(a, b, lane);
+    if (src != nullptr) {
+      const unsigned dst =
+          (unsigned)__cvta_generic_to_shared(reinterpret_cast<unsigned char*>(raw.v) + (PM == kParamsRef32 ? 4 : 8) * lane);
+      if (field_bytes<PM>(a) == 4)
+        asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"(dst), "l"(src) : "memory");
+      else
+        asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(dst), "l"(src) : "memory");
+    }
+  }
+  asm volatile("cp.async.commit_group;" ::: "memory");
+}
+
+// One thread fills a sample's block from its fields (got: GlobalFields or
+// SharedFields); out of line, so that its registers stay out of the pixel loop.
+template <int PM, class Get>
+__device__ __noinline__ void write_block(const KArgs& a, Get got, bool has_qu, SampleBlock& sb) {
+  const SampleRot r = rot_from_fields<PM>(a, got);
+  sb.px = r.px;
+  sb.py = r.py;
+  sb.pz = r.pz;
+  sb.cp = r.cp;
+  sb.sp = r.sp;
+  sb.omp = 1.0 - r.cp;
+  sb.kx = r.kx;
+  sb.ky = r.ky;
+  sb.kz = r.kz;
+  sb.ca = r.ca;
+  sb.sa = r.sa;
+  if constexpr (PM == kParamsRef32) {
+    sb.fkx = r.fkx;
+    sb.fky = r.fky;
+    sb.fkz = r.fkz;
+    sb.fca = r.fca;
+    sb.fsa = r.fsa;
+    sb.oma = 1.0 - (double)r.fca;
+  } else {
+    sb.oma = 1.0 - r.ca;
+  }
+  if (has_qu) {
+    double z, sth, phi;
+    boresight_from_fields<PM>(a, r, got, z, sth, phi);
+    sb.bz = z;
+    sb.bsth = sth;
+    sb.bphi = phi;
+  }
+}
+
+__device__ __forceinline__ unsigned smem_u32(const void* p) { return (unsigned)__cvta_generic_to_shared(p); }
+
+// Shared-memory loads that stay inside the pixel loop (the values are the
+// same for every pixel of a sample; loading them per pixel keeps them out of
+// the registers the evaluation needs).
+__device__ __forceinline__ double2 lds_d2(const void* p) {
+  double2 v;
+  asm volatile("ld.shared.v2.f64 {%0, %1}, [%2];" : "=d"(v.x), "=d"(v.y) : "r"(smem_u32(p)));
+  return v;
+}
+__device__ __forceinline__ double lds_d1(const void* p) {
+  double v;
+  asm volatile("ld.shared.f64 %0, [%1];" : "=d"(v) : "r"(smem_u32(p)));
+  return v;
+}
+__device__ __forceinline__ float4 lds_f4(const void* p) {
+  float4 v;
+  asm volatile("ld.shared.v4.f32 {%0, %1, %2, %3}, [%4];" : "=f"(v.x), "=f"(v.y), "=f"(v.z), "=f"(v.w)
+               : "r"(smem_u32(p)));
+  return v;
+}
+__device__ __forceinline__ int4 lds_i4(const void* p) {
+  int4 v;
+  asm volatile("ld.shared.v4.s32 {%0, %1, %2, %3}, [%4];" : "=r"(v.x), "=r"(v.y), "=r"(v.z), "=r"(v.w)
+               : "r"(smem_u32(p)));
+  return v;
+}
+
+__device__ __forceinline__ Bore block_bore(const SampleBlock* sb) {
+  const double2 zs = lds_d2(&sb->bz);
+  return Bore{zs.x, zs.y, lds_d1(&sb->bphi)};
+}
+
+// Rotated beam pixel with the sample's block: the operations of rot_ref32
+// (float32 parameters, float32 beam vector) or rot_f64 (float64), with 1 - cos a
+// and 1 - cos psi taken from the block (the same values).
+__device__ __forceinline__ void rotate_block(const SampleBlock* sb, float vx, float vy, float vz, double& ox,
+                                             double& oy, double& oz) {
+  const float4 fk = lds_f4(&sb->fkx);  // fkx, fky, fkz, fca
+  const float fsa = lds_f4(&sb->fsa).x;
+  const double oma = lds_d2(&sb->sa).y;
+  const float dkv = fk.x * vx + fk.y * vy + fk.z * vz;
+  const float ax = vx * fk.w + (fk.y * vz - fk.z * vy) * fsa;
+  const float ay = vy * fk.w + (fk.z * vx - fk.x * vz) * fsa;
+  const float az = vz * fk.w + (fk.x * vy - fk.y * vx) * fsa;
+  const double rx = (double)ax + (double)(fk.x * dkv) * oma;
+  const double ry = (double)ay + (double)(fk.y * dkv) * oma;
+  const double rz = (double)az + (double)(fk.z * dkv) * oma;
+  const double2 pxy = lds_d2(&sb->px), pzc = lds_d2(&sb->pz), so = lds_d2(&sb->sp);
+  const double dpr = pxy.x * rx + pxy.y * ry + pzc.x * rz;
+  ox = rx * pzc.y + (pxy.y * rz - pzc.x * ry) * so.x + pxy.x * dpr * so.y;
+  oy = ry * pzc.y + (pzc.x * rx - pxy.x * rz) * so.x + pxy.y * dpr * so.y;
+  oz = rz * pzc.y + (pxy.x * ry - pxy.y * rx) * so.x + pzc.x * dpr * so.y;
+}
+__device__ __forceinline__ void rotate_block(const SampleBlock* sb, double vx, double vy, double vz, double& ox,
+                                             double& oy, double& oz) {
+  const double2 kxy = lds_d2(&sb->kx), kzc = lds_d2(&sb->kz), sao = lds_d2(&sb->sa);
+  const double dkv = kxy.x * vx + kxy.y * vy + kzc.x * vz;
+  const double rx = vx * kzc.y + (kxy.y * vz - kzc.x * vy) * sao.x + kxy.x * dkv * sao.y;
+  const double ry = vy * kzc.y + (kzc.x * vx - kxy.x * vz) * sao.x + kxy.y * dkv * sao.y;
+  const double rz = vz * kzc.y + (kxy.x * vy - kxy.y * vx) * sao.x + kzc.x * dkv * sao.y;
+  const double2 pxy = lds_d2(&sb->px), pzc = lds_d2(&sb->pz), so = lds_d2(&sb->sp);
+  const double dpr = pxy.x * rx + pxy.y * ry + pzc.x * rz;
+  ox = rx * pzc.y + (pxy.y * rz - pzc.x * ry) * so.x + pxy.x * dpr * so.y;
+  oy = ry * pzc.y + (pzc.x * rx - pxy.x * rz) * so.x + pxy.y * dpr * so.y;
+  oz = rz * pzc.y + (pxy.x * ry - pxy.y * rx) * so.x + pzc.x * dpr * so.y;
+}
+
+// The float64 form of the block's rotation applied to a float64 vector (the
+// footprint centre; the operations of rot_f64).
+__device__ __forceinline__ void rotate_block_f64(const SampleBlock& sb, double vx, double vy, double vz, double& ox,
+                                                 double& oy, double& oz) {
+  const double dkv = sb.kx * vx + sb.ky * vy + sb.kz * vz;
+  const double rx = vx * sb.ca + (sb.ky * vz - sb.kz * vy) * sb.sa + sb.kx * dkv * sb.oma;
+  const double ry = vy * sb.ca + (sb.kz * vx - sb.kx * vz) * sb.sa + sb.ky * dkv * sb.oma;
+  const double rz = vz * sb.ca + (sb.kx * vy - sb.ky * vx) * sb.sa + sb.kz * dkv * sb.oma;
+  const double dpr = sb.px * rx + sb.py * ry + sb.pz * rz;
+  ox = rx * sb.cp + (sb.py * rz - sb.pz * ry) * sb.sp + sb.px * dpr * sb.omp;
+  oy = ry * sb.cp + (sb.pz * rx - sb.px * rz) * sb.sp + sb.py * dpr * sb.omp;
+  oz = rz * sb.cp + (sb.px * ry - sb.py * rx) * sb.sp + sb.pz * dpr * sb.omp;
+}
 
 template <typename TabT>
 __device__ __forceinline__ void spin2_lookup(const Spin2Tab& w, const TabT* tab, long long ring, long long ip,
@@ -414,17 +634,15 @@ __device__ __forceinline__ void spin2_lookup(const Spin2Tab& w, const TabT* tab,
   // ip is the pixel's in-ring index and n its ring's length; the spill case
   // (ip == n) and anything outside the window use direct evaluation.
   const long long r = ring - w.ir_lo;
-  if ((unsigned long long)r < (unsigned long long)w.nr && (unsigned long long)ip < (unsigned long long)n) {
-    long long j = ip - w.iplo[r];
+  if ((unsigned long long)r < (unsigned long long)w.hdr.y && (unsigned long long)ip < (unsigned long long)n) {
+    const int4 wr = w.ring[r];
+    long long j = ip - wr.y;
     if (j < 0) j += n;
-    if (j >= 0 && j < w.cap[r]) {
-      const long long slot = w.off[r] + j;
-      if (slot < w.total) {
-        const TabT v = tab[slot];
-        c2d = (double)v.x;
-        s2d = (double)v.y;
-        return;
-      }
+    if (j >= 0 && j < wr.z) {
+      const TabT v = tab[wr.x + j];
+      c2d = (double)v.x;
+      s2d = (double)v.y;
+      return;
     }
   }
   const double sth_n = sqrt(max0(1.0 - zn * zn));
@@ -505,14 +723,139 @@ __device__ void beam_extent(const KArgs& a, double* s_red, double& cx, double& c
   radius = acos(clamp1(mind));
 }
 
+// ---------------------------------------------------------------------------
+// The beam in shared memory.  When the launch leaves room after the spin-2
+// table, each CTA copies its job's beam (pixel vectors and weights, in the
+// caller's layout) there once with bulk copies (cp.async.bulk, 1-D, this
+// GPU's memory, no multicast) on an mbarrier, the unaligned ends of the two
+// arrays with plain loads, and the pixel loop reads it from shared memory.
+// Every wait is bounded: a wait that runs out is counted in
+// g_gather_wait_timeouts (and in the call's error counter), the CTA copies the
+// beam with plain loads instead and waits, again bounded, for the bulk copies
+// it started before going on.
+// ---------------------------------------------------------------------------
+
+constexpr int kStageWaitLimit = 1 << 20;
+__device__ unsigned long long g_gather_wait_timeouts;
+
+// Shared-memory bytes of a staged beam of S pixels with vector elements of
+// vec_elem bytes: each array rounded up to 16 bytes, plus 16 for the offset
+// that keeps a shared copy congruent to its global source modulo 16.
+__host__ __device__ constexpr size_t beam_stage_bytes(long long S, size_t vec_elem) {
+  return (((size_t)(3 * S) * vec_elem + 15) / 16) * 16 + 16 + (((size_t)S * 4 + 15) / 16) * 16 + 16;
+}
+
+__device__ __forceinline__ bool mbar_try_wait(unsigned bar, unsigned parity) {
+  unsigned done;
+  asm volatile("{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\tselp.b32 %0, 1, 0, p;\n\t}"
+               : "=r"(done)
+               : "r"(bar), "r"(parity)
+               : "memory");
+  return done != 0;
+}
+
+__device__ __forceinline__ bool mbar_wait_bounded(unsigned bar, unsigned parity) {
+  for (int it = 0; it < kStageWaitLimit; ++it)
+    if (mbar_try_wait(bar, parity)) return true;
+  return false;
+}
+
+// One array of `count` elements of T at global `src` into shared memory at
+// `region` (16-byte aligned); returns the shared copy's element 0.  Thread 0
+// issues the bulk copy of the 16-byte aligned middle (its bytes are added to
+// `tx`); every thread copies its share of the ends.
+template <typename T, int NT>
+__device__ __forceinline__ T* stage_array(const T* src, long long count, unsigned char* region, unsigned bar,
+                                          unsigned& tx, bool issue) {
+  const unsigned long long g = reinterpret_cast<unsigned long long>(src);
+  const unsigned long long g_end = g + (unsigned long long)count * sizeof(T);
+  const unsigned pad = (unsigned)(g & 15u);
+  T* dst = reinterpret_cast<T*>(region + pad);
+  const unsigned long long body = (g + 15u) & ~15ull, body_end = g_end & ~15ull;
+  // elements [0, head) and [tail0, count) go by plain loads (whole elements:
+  // the source is element-aligned), [head, tail0) by the bulk copy
+  long long head = count, tail0 = count;
+  unsigned bytes = 0;
+  if (body_end > body) {
+    bytes = (unsigned)(body_end - body);
+    head = (long long)((body - g) / sizeof(T));
+    tail0 = (long long)((body_end - g) / sizeof(T));
+  }
+  if (bytes > 0 && issue && threadIdx.x == 0) {
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                     smem_u32(region + pad + (body - g))),
+                 "l"(body), "r"(bytes), "r"(bar)
+                 : "memory");
+  }
+  tx += bytes;
+  const long long ends = head + (count - tail0);
+  for (long long e = threadIdx.x; e < (issue ? ends : count); e += NT) {
+    const long long i = issue ? (e < head ? e : tail0 + (e - head)) : e;
+    dst[i] = src[i];
+  }
+  return dst;
+}
+
+template <typename VecT, int NT>
+__device__ void stage_beam(const KArgs& a, unsigned char* region, unsigned long long* bar_mem, const VecT*& vsrc,
+                           const float*& bsrc) {
+  // (vsrc, bsrc: the shared copies on return)
+  const unsigned bar = smem_u32(bar_mem);
+  const long long S = a.S;
+  unsigned char* vreg = region;
+  unsigned char* breg = region + ((3 * S * sizeof(VecT) + 15) / 16) * 16 + 16;
+  __syncthreads();  // earlier users of the region (the previous job) are done
+  if (threadIdx.x == 0) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(bar) : "memory");
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    // order this CTA's earlier generic-proxy accesses of the region before the
+    // bulk copies' writes
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+  }
+  __syncthreads();
+  // bytes the bulk copies will deliver (the same in every thread)
+  unsigned tx = 0;
+  {
+    const unsigned long long gv = reinterpret_cast<unsigned long long>(a.vec);
+    const unsigned long long gb = reinterpret_cast<unsigned long long>(a.beam);
+    const unsigned long long ve = gv + (unsigned long long)(3 * S) * sizeof(VecT), be = gb + (unsigned long long)S * 4;
+    const unsigned long long vb = (gv + 15) & ~15ull, vbe = ve & ~15ull, bb = (gb + 15) & ~15ull, bbe = be & ~15ull;
+    tx = (unsigned)((vbe > vb ? vbe - vb : 0) + (bbe > bb ? bbe - bb : 0));
+  }
+  if (threadIdx.x == 0 && tx > 0)
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(tx) : "memory");
+  unsigned tx_issued = 0;
+  VecT* sv = stage_array<VecT, NT>(static_cast<const VecT*>(a.vec), 3 * S, vreg, bar, tx_issued, true);
+  float* sbv = stage_array<float, NT>(a.beam, S, breg, bar, tx_issued, true);
+  bool ok = true;
+  if (tx > 0) ok = mbar_wait_bounded(bar, 0);
+  if (!ok) {
+    // the bulk copies did not report back in time: copy everything with plain
+    // loads (the same bytes), then give the copies in flight a last bounded wait
+    if (threadIdx.x == 0) {
+      atomicAdd(&g_gather_wait_timeouts, 1ull);
+      if (a.err != nullptr) atomicAdd(a.err, 1ull);
+    }
+    unsigned dummy = 0;
+    stage_array<VecT, NT>(static_cast<const VecT*>(a.vec), 3 * S, vreg, bar, dummy, false);
+    stage_array<float, NT>(a.beam, S, breg, bar, dummy, false);
+    mbar_wait_bounded(bar, 0);
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) asm volatile("mbarrier.inval.shared::cta.b64 [%0];" ::"r"(bar) : "memory");
+  vsrc = sv;
+  bsrc = sbv;
+}
+
 // One beam pixel's contribution, accumulated into acc[0..3]: generic path
 // (64-bit indices, any ring provider, any component layout).  Used without a
 // ring table and for non-finite rotated vectors.
 template <int MODE, bool HAS_QU, typename MapT, class Rings, typename TabT, class Acc>
-__device__ __noinline__ void eval_generic(const KArgs& a, const Bore& bo, const Rings& rings, const Spin2Tab& w,
-                                          const TabT* tab, double vx, double vy, double vz, double phi_w,
-                                          float bvf, Acc& acc, unsigned long long& nerr) {
+__device__ __noinline__ void eval_generic(const KArgs& a, const SampleBlock* sb, const Rings& rings,
+                                          const Spin2Tab& w, const TabT* tab, double vx, double vy, double vz,
+                                          double phi_w, float bvf, Acc& acc, unsigned long long& nerr) {
   const double bv = (double)bvf;
+  const Bore bo{sb->bz, sb->bsth, sb->bphi};
   if constexpr (MODE == TODGPU_BILINEAR) {
     const double z = clamp1(vz);
     // Per-neighbour terms are summed in the reference's order k = 0..3.
@@ -583,7 +926,8 @@ __device__ __noinline__ void eval_generic(const KArgs& a, const Bore& bo, const 
 // Fast path: finite rotated vector, ring table present, nside <= 8192 (all
 // ring and pixel indices fit 32 bits).  Same decisions and the same floating
 // point operations as the generic path, with 32-bit index arithmetic, ring
-// data from the table and a compile-time component layout.
+// data from the table in 16-byte loads, a compile-time component layout and
+// the spin-2 window looked up once per ring.
 // ---------------------------------------------------------------------------
 
 constexpr int kLayoutGeneric = 0;  // runtime C, c_q, c_u
@@ -596,15 +940,39 @@ struct RingFast {
 
 __device__ __forceinline__ RingFast ring_fast(const RingRec* rt, int ir) {
   const RingRec* r = rt + ir;
+  const double2 zs = __ldg(reinterpret_cast<const double2*>(&r->z));
+  const double2 pd = __ldg(reinterpret_cast<const double2*>(&r->phi0));
+  const double2 ti = __ldg(reinterpret_cast<const double2*>(&r->ta));
+  const int4 fn = __ldg(reinterpret_cast<const int4*>(&r->first32));
   RingFast d;
-  d.n = __ldg(&r->n);
-  d.first = (int)__ldg(&r->first);
-  d.phi0 = __ldg(&r->phi0);
-  d.dphi = __ldg(&r->dphi);
-  d.z = __ldg(&r->z);
-  d.ta = __ldg(&r->ta);
-  d.inv_dphi = __ldg(&r->inv_dphi);
-  d.inv_dta = __ldg(&r->inv_dta);
+  d.z = zs.x;
+  d.phi0 = pd.x;
+  d.dphi = pd.y;
+  d.ta = ti.x;
+  d.inv_dta = ti.y;
+  d.first = fn.x;
+  d.n = fn.y;
+  d.inv_dphi = __longlong_as_double(((long long)(unsigned)fn.w << 32) | (unsigned)fn.z);
+  return d;
+}
+
+// The ring above also needs sin theta of its centre.
+__device__ __forceinline__ RingFast ring_fast_sth(const RingRec* rt, int ir, double& sth) {
+  const RingRec* r = rt + ir;
+  const double2 zs = __ldg(reinterpret_cast<const double2*>(&r->z));
+  const double2 pd = __ldg(reinterpret_cast<const double2*>(&r->phi0));
+  const double2 ti = __ldg(reinterpret_cast<const double2*>(&r->ta));
+  const int4 fn = __ldg(reinterpret_cast<const int4*>(&r->first32));
+  RingFast d;
+  d.z = zs.x;
+  sth = zs.y;
+  d.phi0 = pd.x;
+  d.dphi = pd.y;
+  d.ta = ti.x;
+  d.inv_dta = ti.y;
+  d.first = fn.x;
+  d.n = fn.y;
+  d.inv_dphi = __longlong_as_double(((long long)(unsigned)fn.w << 32) | (unsigned)fn.z);
   return d;
 }
 
@@ -647,13 +1015,59 @@ __device__ __forceinline__ double div_rn(double x, double d, double y) {
 }
 constexpr double kInvTwoPi = 1.0 / kTwoPi;
 
+// Spin-2 window entry of one ring of the sample: {off, iplo, cap} and
+// whether the ring lies in the window.
+struct RingWin {
+  int off, iplo, cap;
+  bool in;
+};
+
+__device__ __forceinline__ int2 lds_i2(const void* p) {
+  int2 v;
+  asm volatile("ld.shared.v2.s32 {%0, %1}, [%2];" : "=r"(v.x), "=r"(v.y) : "r"(smem_u32(p)));
+  return v;
+}
+
+__device__ __forceinline__ RingWin ring_win(const Spin2Tab& w, const int2& hdr, int ring) {
+  const unsigned r = (unsigned)(ring - hdr.x);
+  RingWin rw;
+  rw.in = r < (unsigned)hdr.y;
+  const int4 v = lds_i4(&w.ring[rw.in ? r : 0u]);
+  rw.off = v.x;
+  rw.iplo = v.y;
+  rw.cap = v.z;
+  return rw;
+}
+
+// cos 2d / sin 2d of in-ring pixel ip (of n) from the table, or directly
+// (pixel outside the window, spill case ip == n).
+template <typename TabT>
+__device__ __forceinline__ void spin2_win(const RingWin& rw, const TabT* tab, const SampleBlock* sb, int ip, int n,
+                                          double zn, double phin, double& c2d, double& s2d) {
+  int j = ip - rw.iplo;
+  j += (j >> 31) & n;
+  if (rw.in && (unsigned)ip < (unsigned)n && (unsigned)j < (unsigned)rw.cap) {
+    const TabT v = tab[rw.off + j];
+    c2d = (double)v.x;
+    s2d = (double)v.y;
+    return;
+  }
+  const Bore bo = block_bore(sb);
+  const double sth_n = sqrt(max0(1.0 - zn * zn));
+  spin2_c2s2(zn, sth_n, phin, bo.z, bo.sth, bo.phi, c2d, s2d);
+}
+
 // The bilinear stencil of hp_stencil with 32-bit indices; tw is in [0, n]
-// for finite phi in [0, 2 pi], so int(tw) is a plain truncation.
-template <class Visit>
-__device__ __forceinline__ void stencil_fast(int nside, double z, double phi_w, const RingRec* rt, Visit&& visit) {
+// for finite phi in [0, 2 pi], so int(tw) is a plain truncation.  visit(k,
+// pixel, weight, in-ring index, ring length, ring z, pixel phi, ring window).
+template <bool HAS_QU, class Visit>
+__device__ __forceinline__ void stencil_fast(int nside, double z, double phi_w, const RingRec* rt, const Spin2Tab& w,
+                                             const int2& hdr, Visit&& visit) {
   const int ir_above = ring_above_fast(nside, z);
+  RingWin ra_w{0, 0, 0, false};
   if (ir_above == 0) {
     const RingFast ra = ring_fast(rt, 1);
+    if constexpr (HAS_QU) ra_w = ring_win(w, hdr, 1);
     const double tw = py_fmod_pos((phi_w - ra.phi0) / ra.dphi, (double)ra.n);
     const int ip = (int)tw;
     const double frac = tw - (double)ip;
@@ -662,13 +1076,14 @@ __device__ __forceinline__ void stencil_fast(int nside, double z, double phi_w, 
     const double theta = acos(z);
     const double wt = theta / ra.ta;
     const double nf = (1.0 - wt) * 0.25;
-    visit(0, ra.first + o1, nf, 1, o1, ra.n, ra.z, ra.phi0 + (double)o1 * ra.dphi);
-    visit(1, ra.first + o2, nf, 1, o2, ra.n, ra.z, ra.phi0 + (double)o2 * ra.dphi);
-    visit(2, ra.first + ip, (1.0 - frac) * wt + nf, 1, ip, ra.n, ra.z, ra.phi0 + (double)ip * ra.dphi);
-    visit(3, ra.first + ip2, frac * wt + nf, 1, ip2, ra.n, ra.z, ra.phi0 + (double)ip2 * ra.dphi);
+    visit(0, ra.first + o1, nf, o1, ra.n, ra.z, ra.phi0 + (double)o1 * ra.dphi, ra_w);
+    visit(1, ra.first + o2, nf, o2, ra.n, ra.z, ra.phi0 + (double)o2 * ra.dphi, ra_w);
+    visit(2, ra.first + ip, (1.0 - frac) * wt + nf, ip, ra.n, ra.z, ra.phi0 + (double)ip * ra.dphi, ra_w);
+    visit(3, ra.first + ip2, frac * wt + nf, ip2, ra.n, ra.z, ra.phi0 + (double)ip2 * ra.dphi, ra_w);
   } else if (ir_above == 4 * nside - 1) {
     const int ir_last = 4 * nside - 1;
     const RingFast ra = ring_fast(rt, ir_last);
+    if constexpr (HAS_QU) ra_w = ring_win(w, hdr, ir_last);
     const double tw = py_fmod_pos((phi_w - ra.phi0) / ra.dphi, (double)ra.n);
     const int ip = (int)tw;
     const double frac = tw - (double)ip;
@@ -677,51 +1092,38 @@ __device__ __forceinline__ void stencil_fast(int nside, double z, double phi_w, 
     const double theta = acos(z);
     const double ws = (theta - ra.ta) / (kPi - ra.ta);
     const double sf = ws * 0.25;
-    visit(0, ra.first + ip, (1.0 - frac) * (1.0 - ws) + sf, ir_last, ip, ra.n, ra.z, ra.phi0 + (double)ip * ra.dphi);
-    visit(1, ra.first + ip2, frac * (1.0 - ws) + sf, ir_last, ip2, ra.n, ra.z, ra.phi0 + (double)ip2 * ra.dphi);
-    visit(2, ra.first + o1, sf, ir_last, o1, ra.n, ra.z, ra.phi0 + (double)o1 * ra.dphi);
-    visit(3, ra.first + o2, sf, ir_last, o2, ra.n, ra.z, ra.phi0 + (double)o2 * ra.dphi);
+    visit(0, ra.first + ip, (1.0 - frac) * (1.0 - ws) + sf, ip, ra.n, ra.z, ra.phi0 + (double)ip * ra.dphi, ra_w);
+    visit(1, ra.first + ip2, frac * (1.0 - ws) + sf, ip2, ra.n, ra.z, ra.phi0 + (double)ip2 * ra.dphi, ra_w);
+    visit(2, ra.first + o1, sf, o1, ra.n, ra.z, ra.phi0 + (double)o1 * ra.dphi, ra_w);
+    visit(3, ra.first + o2, sf, o2, ra.n, ra.z, ra.phi0 + (double)o2 * ra.dphi, ra_w);
   } else {
     const int ir_below = ir_above + 1;
-    const RingFast ra = ring_fast(rt, ir_above);
-    const RingFast rb = ring_fast(rt, ir_below);
+    double sth_a;
+    const RingFast ra = ring_fast_sth(rt, ir_above, sth_a);
+    // of the ring below only its colatitude is needed before the ring above's
+    // neighbours; the rest is loaded after them
+    const double ta_b = __ldg(&rt[ir_below].ta);
     double dta;
-    if (!dtheta_small(z, ra.z, __ldg(&rt[ir_above].sth), dta)) dta = acos(z) - ra.ta;
-    const double wb = div_rn(dta, rb.ta - ra.ta, ra.inv_dta);
+    if (!dtheta_small(z, ra.z, sth_a, dta)) dta = acos(z) - ra.ta;
+    const double wb = div_rn(dta, ta_b - ra.ta, ra.inv_dta);
     const double wa = 1.0 - wb;
     double tw = py_fmod_pos(div_rn(phi_w - ra.phi0, ra.dphi, ra.inv_dphi), (double)ra.n);
     const int ia = (int)tw;
     const double fa = tw - (double)ia;
     const int ia1 = wrap_up(ia, 1, ra.n);
-    visit(0, ra.first + ia, wa * (1.0 - fa), ir_above, ia, ra.n, ra.z, ra.phi0 + (double)ia * ra.dphi);
-    visit(1, ra.first + ia1, wa * fa, ir_above, ia1, ra.n, ra.z, ra.phi0 + (double)ia1 * ra.dphi);
+    if constexpr (HAS_QU) ra_w = ring_win(w, hdr, ir_above);
+    visit(0, ra.first + ia, wa * (1.0 - fa), ia, ra.n, ra.z, ra.phi0 + (double)ia * ra.dphi, ra_w);
+    visit(1, ra.first + ia1, wa * fa, ia1, ra.n, ra.z, ra.phi0 + (double)ia1 * ra.dphi, ra_w);
+    const RingFast rb = ring_fast(rt, ir_below);
     tw = py_fmod_pos(div_rn(phi_w - rb.phi0, rb.dphi, rb.inv_dphi), (double)rb.n);
     const int ib = (int)tw;
     const double fb = tw - (double)ib;
     const int ib1 = wrap_up(ib, 1, rb.n);
-    visit(2, rb.first + ib, wb * (1.0 - fb), ir_below, ib, rb.n, rb.z, rb.phi0 + (double)ib * rb.dphi);
-    visit(3, rb.first + ib1, wb * fb, ir_below, ib1, rb.n, rb.z, rb.phi0 + (double)ib1 * rb.dphi);
+    RingWin rb_w{0, 0, 0, false};
+    if constexpr (HAS_QU) rb_w = ring_win(w, hdr, ir_below);
+    visit(2, rb.first + ib, wb * (1.0 - fb), ib, rb.n, rb.z, rb.phi0 + (double)ib * rb.dphi, rb_w);
+    visit(3, rb.first + ib1, wb * fb, ib1, rb.n, rb.z, rb.phi0 + (double)ib1 * rb.dphi, rb_w);
   }
-}
-
-// Table lookup with 32-bit indices (ip == n is the spill case: direct).
-template <typename TabT>
-__device__ __forceinline__ void spin2_fast(const Spin2Tab& w, const TabT* tab, int ring, int ip, int n, double zn,
-                                           double phin, const Bore& bo, double& c2d, double& s2d) {
-  const unsigned r = (unsigned)(ring - w.ir_lo32);
-  if (r < (unsigned)w.nr && (unsigned)ip < (unsigned)n) {
-    int j = ip - w.iplo[r];
-    j += (j >> 31) & n;
-    const int slot = w.off[r] + j;
-    if ((unsigned)j < (unsigned)w.cap[r] && slot < w.total) {
-      const TabT v = tab[slot];
-      c2d = (double)v.x;
-      s2d = (double)v.y;
-      return;
-    }
-  }
-  const double sth_n = sqrt(max0(1.0 - zn * zn));
-  spin2_c2s2(zn, sth_n, phin, bo.z, bo.sth, bo.phi, c2d, s2d);
 }
 
 template <int LAYOUT>
@@ -776,25 +1178,41 @@ struct PixelVals<PackF64> {
   }
 };
 
+// The nearest rule's ring data: n, phi0, dphi, z and sin theta of ring ir.
+struct RingNear {
+  int n, first;
+  double phi0, dphi, z, sth;
+};
+__device__ __forceinline__ RingNear ring_near(const RingRec* rt, int ir) {
+  const RingRec* r = rt + ir;
+  const double2 zs = __ldg(reinterpret_cast<const double2*>(&r->z));
+  const double2 pd = __ldg(reinterpret_cast<const double2*>(&r->phi0));
+  const int2 fn = __ldg(reinterpret_cast<const int2*>(&r->first32));
+  return RingNear{fn.y, fn.x, pd.x, pd.y, zs.x, zs.y};
+}
+
 template <int MODE, bool HAS_QU, typename MapT, int LAYOUT, typename TabT, class Acc>
-__device__ __forceinline__ void eval_fast(const KArgs& a, const Bore& bo, const RingRec* rt, const Spin2Tab& w,
-                                          const TabT* tab, double vx, double vy, double vz, double phi_w,
-                                          float bvf, Acc& acc) {
+__device__ __forceinline__ void eval_fast(const KArgs& a, const SampleBlock* sb, const RingRec* rt,
+                                          const Spin2Tab& w, const TabT* tab, double vx, double vy, double vz,
+                                          double phi_w, float bvf, Acc& acc) {
   constexpr bool kPacked = MapTraits<MapT>::packed;
   const Chan<LAYOUT> ch(a);
   const int nside = (int)a.nside;
   const double bv = (double)bvf;
+  int2 hdr = make_int2(0, 0);  // {first window ring, window rings}
+  if constexpr (HAS_QU) hdr = lds_i2(&w.hdr);
   if constexpr (MODE == TODGPU_BILINEAR) {
     const double z = clamp1(vz);
     if constexpr (kPacked) {
       // precision form: one record per neighbour, float32 mixing
       float tq = 0.f, tu = 0.f, to[4] = {0.f, 0.f, 0.f, 0.f};
-      stencil_fast(nside, z, phi_w, rt, [&](int k, int p, double wk, int ring, int ip, int n, double zn, double phin) {
+      stencil_fast<HAS_QU>(nside, z, phi_w, rt, w, hdr,
+                           [&](int k, int p, double wk, int ip, int n, double zn, double phin, const RingWin& rw) {
         const float4 rec = load_rec<MapT>(a, p);
         const float wf = (float)wk;
         if constexpr (HAS_QU) {
           double c2, s2;
-          spin2_fast(w, tab, ring, ip, n, zn, phin, bo, c2, s2);
+          spin2_win(rw, tab, sb, ip, n, zn, phin, c2, s2);
           const float c2f = (float)c2, s2f = (float)s2;
           const float q = rec_at(rec, ch.q), u = rec_at(rec, ch.u);
           const float vq = wf * fmaf(q, c2f, u * s2f);
@@ -821,11 +1239,12 @@ __device__ __forceinline__ void eval_fast(const KArgs& a, const Bore& bo, const 
       }
     } else {
       double tq = 0.0, tu = 0.0, to[4] = {0.0, 0.0, 0.0, 0.0};
-      stencil_fast(nside, z, phi_w, rt, [&](int k, int p, double wk, int ring, int ip, int n, double zn, double phin) {
+      stencil_fast<HAS_QU>(nside, z, phi_w, rt, w, hdr,
+                           [&](int k, int p, double wk, int ip, int n, double zn, double phin, const RingWin& rw) {
         const PixelVals<MapT> pv(a, p);
         if constexpr (HAS_QU) {
           double c2, s2;
-          spin2_fast(w, tab, ring, ip, n, zn, phin, bo, c2, s2);
+          spin2_win(rw, tab, sb, ip, n, zn, phin, c2, s2);
           const double q = pv(ch.q);
           const double u = pv(ch.u);
           const double vq = wk * fma(q, c2, u * s2);
@@ -871,26 +1290,24 @@ __device__ __forceinline__ void eval_fast(const KArgs& a, const Bore& bo, const 
     // picks.  A closer call is ranked again by cos() itself -- the same
     // expression, order and strict comparison -- so the pixel is always the
     // one of ranking by cos() throughout.
-    int best_ring = -1, best_ip = 0;
+    int best_g = -1, best_ip = 0;
+    const RingNear rg0 = ring_near(rt, ir_above), rg1 = ring_near(rt, ir_above + 1);
     {
       double lead = -3.0, runner = -3.0;
 #pragma unroll
       for (int g = 0; g < 2; ++g) {
-        const int ir = ir_above + g;
-        const RingRec* rr = rt + ir;
-        const int n = __ldg(&rr->n);
-        const double phi0 = __ldg(&rr->phi0), dphi = __ldg(&rr->dphi), zc = __ldg(&rr->z), szc = __ldg(&rr->sth);
-        int ipb = (int)div_rn(phi_w * (double)n, kTwoPi, kInvTwoPi);
-        if (ipb >= n) ipb -= n;
+        const RingNear& r = g == 0 ? rg0 : rg1;
+        int ipb = (int)div_rn(phi_w * (double)r.n, kTwoPi, kInvTwoPi);
+        if (ipb >= r.n) ipb -= r.n;
 #pragma unroll
         for (int t = 0; t < 2; ++t) {
-          const int ip = (t == 0) ? ipb : wrap_up(ipb, 1, n);
-          const double dl = phi_w - (phi0 + (double)ip * dphi);
-          const double cosd = sin_th * szc * (fabs(dl) <= kCosSmallMax ? cos_small(dl) : cos(dl)) + vz * zc;
+          const int ip = (t == 0) ? ipb : wrap_up(ipb, 1, r.n);
+          const double dl = phi_w - (r.phi0 + (double)ip * r.dphi);
+          const double cosd = sin_th * r.sth * (fabs(dl) <= kCosSmallMax ? cos_small(dl) : cos(dl)) + vz * r.z;
           if (cosd > lead) {
             runner = lead;
             lead = cosd;
-            best_ring = ir;
+            best_g = g;
             best_ip = ip;
           } else if (cosd > runner) {
             runner = cosd;
@@ -899,47 +1316,46 @@ __device__ __forceinline__ void eval_fast(const KArgs& a, const Bore& bo, const 
       }
       if (!(lead - runner > 1e-13)) {
         double best_cos = -2.0;
-        best_ring = -1;
+        best_g = -1;
 #pragma unroll
         for (int g = 0; g < 2; ++g) {
-          const int ir = ir_above + g;
-          const RingRec* rr = rt + ir;
-          const int n = __ldg(&rr->n);
-          const double phi0 = __ldg(&rr->phi0), dphi = __ldg(&rr->dphi), zc = __ldg(&rr->z), szc = __ldg(&rr->sth);
-          int ipb = (int)(phi_w * (double)n / kTwoPi);
-          if (ipb >= n) ipb -= n;
+          const RingNear& r = g == 0 ? rg0 : rg1;
+          int ipb = (int)(phi_w * (double)r.n / kTwoPi);
+          if (ipb >= r.n) ipb -= r.n;
 #pragma unroll
           for (int t = 0; t < 2; ++t) {
-            const int ip = (t == 0) ? ipb : wrap_up(ipb, 1, n);
-            const double phic = phi0 + (double)ip * dphi;
-            const double cosd = sin_th * szc * cos(phi_w - phic) + vz * zc;
+            const int ip = (t == 0) ? ipb : wrap_up(ipb, 1, r.n);
+            const double phic = r.phi0 + (double)ip * r.dphi;
+            const double cosd = sin_th * r.sth * cos(phi_w - phic) + vz * r.z;
             if (cosd > best_cos) {
               best_cos = cosd;
-              best_ring = ir;
+              best_g = g;
               best_ip = ip;
             }
           }
         }
       }
     }
-    int best_pix = 0, best_n = 1;
+    int best_pix = 0, best_n = 1, best_ring = 0;
     double best_zc = 0.0, best_phic = 0.0;
-    if (best_ring >= 0) {
-      const RingRec* rr = rt + best_ring;
-      best_n = __ldg(&rr->n);
-      best_pix = (int)__ldg(&rr->first) + best_ip;
-      best_zc = __ldg(&rr->z);
-      best_phic = __ldg(&rr->phi0) + (double)best_ip * __ldg(&rr->dphi);
+    if (best_g >= 0) {
+      const RingNear& r = best_g == 0 ? rg0 : rg1;
+      best_ring = ir_above + best_g;
+      best_n = r.n;
+      best_pix = r.first + best_ip;
+      best_zc = r.z;
+      best_phic = r.phi0 + (double)best_ip * r.dphi;
     } else {
-      best_ring = 0;
       best_ip = 0;
     }
+    RingWin rw{0, 0, 0, false};
+    if constexpr (HAS_QU) rw = ring_win(w, hdr, best_ring);
     if constexpr (kPacked) {
       const float4 rec = load_rec<MapT>(a, best_pix);
       float c2f = 1.f, s2f = 0.f;
       if constexpr (HAS_QU) {
         double c2d, s2d;
-        spin2_fast(w, tab, best_ring, best_ip, best_n, best_zc, best_phic, bo, c2d, s2d);
+        spin2_win(rw, tab, sb, best_ip, best_n, best_zc, best_phic, c2d, s2d);
         c2f = (float)c2d;
         s2f = (float)s2d;
       }
@@ -955,7 +1371,7 @@ __device__ __forceinline__ void eval_fast(const KArgs& a, const Bore& bo, const 
       }
     } else if constexpr (HAS_QU) {
       double c2d, s2d;
-      spin2_fast(w, tab, best_ring, best_ip, best_n, best_zc, best_phic, bo, c2d, s2d);
+      spin2_win(rw, tab, sb, best_ip, best_n, best_zc, best_phic, c2d, s2d);
       const double qv = map_i<MapT>(a, ch.q, best_pix);
       const double uv = map_i<MapT>(a, ch.u, best_pix);
 #pragma unroll
@@ -1032,8 +1448,8 @@ static __device__ __noinline__ void footprint_window(const KArgs& a, const RingR
         const double c = floor((phi_u - __ldg(&r->phi0)) / __ldg(&r->dphi));
         iplo = (int)py_imod((long long)c - (cnt - 1) / 2, n);
       }
-      w.iplo[t] = iplo;
-      w.cap[t] = cnt;
+      w.ring[t].y = iplo;
+      w.ring[t].z = cnt;
     }
   }
   // slot offsets: exclusive prefix sum of the counts, by warp 0 once both
@@ -1044,23 +1460,21 @@ static __device__ __noinline__ void footprint_window(const KArgs& a, const RingR
     if (fits) {
       for (int b0 = 0; b0 < (int)nr; b0 += 32) {
         const int t = b0 + lane;
-        const int own = t < nr ? w.cap[t] : 0;
+        const int own = t < nr ? w.ring[t].z : 0;
         int v = own;
 #pragma unroll
         for (int o = 1; o < 32; o <<= 1) {
           const int y = __shfl_up_sync(0xffffffffu, v, o);
           if (lane >= o) v += y;
         }
-        if (t < nr) w.off[t] = carry + v - own;
+        if (t < nr) w.ring[t].x = carry + v - own;
         carry += __shfl_sync(0xffffffffu, v, 31);
       }
     }
     fits = fits && carry <= a.tab_cap;
     if (threadIdx.x == 0) {
       w.ir_lo = ir_lo;
-      w.ir_lo32 = (int)ir_lo;
-      w.nr = fits ? (int)nr : 0;
-      w.total = fits ? carry : 0;
+      w.hdr = make_int4((int)ir_lo, fits ? (int)nr : 0, fits ? carry : 0, 0);
     }
   }
 }
@@ -1070,7 +1484,11 @@ static __device__ __noinline__ void footprint_window(const KArgs& a, const RingR
 // min(B, (t + 1) tile))), by the whole CTA.  With a ring table:
 // ring data come from it and, when the entry carries Q and U, each sample's
 // footprint gets a spin-2 table in shared memory.  Without one: everything is
-// evaluated directly.  All threads of the CTA must call it together.
+// evaluated directly.  Each sample's rotation and boresight are derived by one
+// thread, one sample ahead, into a double-buffered shared block that all
+// threads read.  The beam is read from shared memory when the launch staged
+// it there (a.beam_stage), else from global memory.  All threads of the CTA
+// must call it together.
 template <int MODE, bool HAS_QU, typename MapT, int PM, int LAYOUT, int NT>
 __device__ void run_samples(const KArgs& a, long long t_begin, long long t_end, long long t_step, long long tile,
                             unsigned char* smem_raw, double* s_red) {
@@ -1078,7 +1496,10 @@ __device__ void run_samples(const KArgs& a, long long t_begin, long long t_end, 
   Spin2Tab& w = *reinterpret_cast<Spin2Tab*>(smem_raw);
   using TabT = typename MapTraits<MapT>::Tab;
   using Acc = typename std::conditional<MapTraits<MapT>::packed, AccKahan, Acc64>::type;
+  using VecT = typename std::conditional<PM == kParamsRef32, float, double>::type;
   TabT* tab = reinterpret_cast<TabT*>(smem_raw + ((sizeof(Spin2Tab) + 15) & ~size_t(15)));
+  __shared__ SampleBlock s_blk[2];
+  __shared__ __align__(8) unsigned long long s_bar;
 
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const RingRec* rt = static_cast<const RingRec*>(a.ring_table);
@@ -1098,68 +1519,66 @@ __device__ void run_samples(const KArgs& a, long long t_begin, long long t_end, 
     use_tab = reach <= __ldg(&rt[0].ta);
   }
   if (threadIdx.x == 0) {
-    w.nr = 0;
-    w.total = 0;
+    w.hdr = make_int4(0, 0, 0, 0);
     w.ir_lo = 0;
-    w.ir_lo32 = 0;
   }
-  // Angles mode: one thread derives each sample's rotation and boresight, one
-  // sample ahead, into a double-buffered shared slot instead of every thread
-  // computing the same values -- the last thread, which has the fewest beam
-  // pixels when S is not a multiple of the CTA size.  The shared float64
-  // parameter mode (chosen by the host for large beams, where every thread's
-  // boresight atan2 costs more than one thread's serial load-and-atan2 chain)
-  // does the same with loaded parameters.  Other modes load their per-sample
-  // parameters in every thread (a few cached loads).
-  constexpr bool kShareRot = (PM == kAngles || PM == kParamsF64Shared);
+  const VecT* svec = nullptr;
+  const float* sbv = nullptr;
+  const bool staged = a.beam_stage != 0;
+  if (staged) {
+    const size_t off = ((sizeof(Spin2Tab) + 15) & ~size_t(15)) + (((size_t)a.tab_cap * sizeof(TabT) + 15) & ~size_t(15));
+    stage_beam<VecT, NT>(a, smem_raw + off, &s_bar, svec, sbv);
+  }
+  // one thread derives each sample's rotation and boresight, one sample ahead:
+  // the last thread, which has the fewest beam pixels when S is not a multiple
+  // of the CTA size
   constexpr int kRotThread = NT - 1;
-  __shared__ SampleRot s_rot[2];
-  __shared__ Bore s_bo[2];
-  if constexpr (kShareRot) {
-    if (threadIdx.x == kRotThread && t_begin < t_end) {
-      const long long b0 = t_begin * tile;
-      s_rot[0] = load_rot<PM>(a, b0);
-      if (HAS_QU) load_boresight<PM>(a, s_rot[0], b0, s_bo[0].z, s_bo[0].sth, s_bo[0].phi);
-    }
-  }
+  constexpr int kRotWarp = NW - 1;
+  __shared__ RawFields s_raw;
+  if (threadIdx.x == kRotThread && t_begin < t_end)
+    write_block<PM>(a, GlobalFields<PM>{a, t_begin * tile}, HAS_QU, s_blk[0]);
   int slot = 0;
   unsigned long long nerr = 0;
   long long prev = -1;
+  const int S = (int)a.S;
   for (long long t = t_begin; t < t_end; t += t_step)
   for (long long b = t * tile, b_stop = min(a.B, (t + 1) * tile); b < b_stop; ++b) {
-    SampleRot rot;
-    Bore bo{0.0, 0.0, 0.0};
-    if constexpr (!kShareRot) {
-      rot = load_rot<PM>(a, b);
-      if (HAS_QU) load_boresight<PM>(a, rot, b, bo.z, bo.sth, bo.phi);
+    __syncthreads();  // previous sample is done with the table, its partial sums and its block
+    const SampleBlock* sb = &s_blk[slot];
+    // the next sample: its pointing fields start on their way to shared memory
+    // now, and the last thread turns them into its block after its pixels
+    long long bn = b + 1, tn = t;
+    if (bn >= b_stop) {
+      tn = t + t_step;
+      bn = tn * tile;
     }
-    __syncthreads();  // previous sample is done with the table, its partial sums and its slot
-    if constexpr (kShareRot) {
-      rot = s_rot[slot];
-      if (HAS_QU) bo = s_bo[slot];
-    }
+    const bool has_next = tn < t_end && bn < a.B;
+    if (warp == kRotWarp && has_next) prefetch_fields<PM>(a, bn, s_raw, lane);
     if (prev >= 0 && threadIdx.x == 0) flush_sample<NW>(a, s_red, prev);
     if (use_tab) {
       if (threadIdx.x < kSetupThreads) {
         // footprint window of this sample (same values in every setup thread)
         double ux, uy, uz;
-        rot_f64(rot, cx, cy, cz, ux, uy, uz);
+        rotate_block_f64(*sb, cx, cy, cz, ux, uy, uz);
         footprint_window(a, rt, w, ux, uy, uz, reach);
       }
       __syncthreads();
-      const int ntab = w.total, nwin = w.nr;
+      const int4 hdr = w.hdr;
+      const int ntab = hdr.z, nwin = hdr.y;
+      const Bore bo{sb->bz, sb->bsth, sb->bphi};
       for (int e = threadIdx.x; e < ntab; e += NT) {
         int lo = 0, hi = nwin - 1;  // last window ring with off <= e
         while (lo < hi) {
           const int mid = (lo + hi + 1) >> 1;
-          if (w.off[mid] <= e)
+          if (w.ring[mid].x <= e)
             lo = mid;
           else
             hi = mid - 1;
         }
+        const int4 wr = w.ring[lo];
         const RingRec* r = rt + w.ir_lo + lo;
         const int n = __ldg(&r->n);
-        int ip = w.iplo[lo] + (e - w.off[lo]);
+        int ip = wr.y + (e - wr.x);
         if (ip >= n) ip -= n;
         const double phin = __ldg(&r->phi0) + (double)ip * __ldg(&r->dphi);
         double c2, s2;
@@ -1170,19 +1589,32 @@ __device__ void run_samples(const KArgs& a, long long t_begin, long long t_end, 
     __syncthreads();
 
     Acc acc;
-    for (long long s = threadIdx.x; s < a.S; s += NT) {
+    for (int s = threadIdx.x; s < S; s += NT) {
+      VecT v0, v1, v2;
+      float bvf;
+      if (staged) {
+        v0 = svec[3 * s];
+        v1 = svec[3 * s + 1];
+        v2 = svec[3 * s + 2];
+        bvf = sbv[s];
+      } else {
+        const VecT* v = static_cast<const VecT*>(a.vec) + 3 * s;
+        v0 = __ldg(v);
+        v1 = __ldg(v + 1);
+        v2 = __ldg(v + 2);
+        bvf = __ldg(a.beam + s);
+      }
       double vx, vy, vz;
-      rotate_pixel<PM>(a, rot, s, vx, vy, vz);
-      const float bvf = __ldg(a.beam + s);
+      rotate_block(sb, v0, v1, v2, vx, vy, vz);
       double phi_w = atan2(vy, vx);
       if (phi_w < 0.0) phi_w += kTwoPi;
       if (fast && isfinite(vx) && isfinite(vy) && isfinite(vz)) {
-        eval_fast<MODE, HAS_QU, MapT, LAYOUT>(a, bo, rt, w, tab, vx, vy, vz, phi_w, bvf, acc);
+        eval_fast<MODE, HAS_QU, MapT, LAYOUT>(a, sb, rt, w, tab, vx, vy, vz, phi_w, bvf, acc);
       } else if (rt != nullptr) {
-        eval_generic<MODE, HAS_QU, MapT>(a, bo, TableRings{rt}, w, tab, vx, vy, vz, phi_w, bvf, acc, nerr);
+        eval_generic<MODE, HAS_QU, MapT>(a, sb, TableRings{rt}, w, tab, vx, vy, vz, phi_w, bvf, acc, nerr);
       } else {
-        eval_generic<MODE, HAS_QU, MapT>(a, bo, DirectRings{a.nside, a.npix}, w, tab, vx, vy, vz, phi_w, bvf,
-                                         acc, nerr);
+        eval_generic<MODE, HAS_QU, MapT>(a, sb, DirectRings{a.nside, a.npix}, w, tab, vx, vy, vz, phi_w, bvf, acc,
+                                         nerr);
       }
     }
 #pragma unroll
@@ -1191,22 +1623,13 @@ __device__ void run_samples(const KArgs& a, long long t_begin, long long t_end, 
       const double v = warp_sum(acc.total(c));
       if (lane == 0) s_red[warp * 4 + c] = v;
     }
-    if constexpr (kShareRot) {
-      // the next sample's rotation into the other slot (read after the next barrier)
-      if (threadIdx.x == kRotThread) {
-        long long bn = b + 1, tn = t;
-        if (bn >= b_stop) {
-          tn = t + t_step;
-          bn = tn * tile;
-        }
-        if (tn < t_end && bn < a.B) {
-          s_rot[slot ^ 1] = load_rot<PM>(a, bn);
-          if (HAS_QU) load_boresight<PM>(a, s_rot[slot ^ 1], bn, s_bo[slot ^ 1].z, s_bo[slot ^ 1].sth,
-                                         s_bo[slot ^ 1].phi);
-        }
-      }
-      slot ^= 1;
+    // the next sample's rotation into the other block (read after the next barrier)
+    if (warp == kRotWarp && has_next) {
+      asm volatile("cp.async.wait_all;" ::: "memory");
+      __syncwarp();
+      if (lane == 31) write_block<PM>(a, SharedFields<PM>{a, s_raw}, HAS_QU, s_blk[slot ^ 1]);
     }
+    slot ^= 1;
     prev = b;
   }
   __syncthreads();
@@ -1216,7 +1639,7 @@ __device__ void run_samples(const KArgs& a, long long t_begin, long long t_end, 
     for (int o = 16; o > 0; o >>= 1) nerr += __shfl_xor_sync(0xffffffffu, nerr, o);
     if (lane == 0 && nerr) atomicAdd(a.err, nerr);
   }
-  __syncthreads();  // the partial sums and tables may be reused by the next job
+  __syncthreads();  // the partial sums, tables and blocks may be reused by the next job
 }
 
 template <int MODE, bool HAS_QU, typename MapT, int PM, int LAYOUT, int NT, int MINB>
@@ -1291,10 +1714,6 @@ constexpr size_t kTabHeaderBytes = (sizeof(Spin2Tab) + 15) & ~size_t(15);
 #define TODGPU_CTA_THREADS 256
 #endif
 constexpr int kNT = TODGPU_CTA_THREADS;  // threads per CTA
-// Beams of at least this many pixels (16 per thread) take the shared float64
-// parameter mode in the single-launch kernel (measured: S = 9530 runs 3-6%
-// faster shared; S = 1512 runs 8-11% slower shared, hence the threshold).
-constexpr long long kShareRotMinS = 16LL * kNT;
 
 // CTAs per SM the register budget is sized for: 4 (64 registers) for the
 // nearest mode and packed maps, where the fourth CTA measured 3-5% faster; 3
@@ -1316,6 +1735,14 @@ template <typename TabT, int MINB>
 constexpr int max_table_slots() {
   return (int)((kSmemPerSM / MINB - kSmemPerCTAReserved - kStaticSmemMargin - kTabHeaderBytes) / sizeof(TabT));
 }
+constexpr size_t align16(size_t x) { return (x + 15) & ~size_t(15); }
+
+// Dynamic shared memory a CTA may take while MINB CTAs still fit on an SM.
+template <int MINB>
+constexpr size_t cta_smem_budget() {
+  return kSmemPerSM / MINB - kSmemPerCTAReserved - kStaticSmemMargin;
+}
+
 template <typename TabT, int MINB>
 int table_slots(int requested) {
   constexpr int kCap = (int)(kTabCapDefault * sizeof(double2) / sizeof(TabT));
@@ -1326,12 +1753,16 @@ int table_slots(int requested) {
 // launch's shared memory (recomputed when it changes).
 template <typename TabT, int MINB, typename Kern>
 int configure_launch(Kern kern, LaunchInfo& info, std::mutex& mu, size_t smem, int& blocks_per_sm) {
-  constexpr int kCap = (int)(kTabCapDefault * sizeof(double2) / sizeof(TabT));
-  constexpr size_t smem_limit =
-      kTabHeaderBytes + sizeof(TabT) * (size_t)std::max(kCap, max_table_slots<TabT, MINB>());
   std::lock_guard<std::mutex> lock(mu);
   if (!info.configured) {
-    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_limit);
+    // the largest dynamic shared memory a CTA of this kernel can have
+    int dev = 0, optin = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e == cudaSuccess) e = cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+    cudaFuncAttributes fa;
+    if (e == cudaSuccess) e = cudaFuncGetAttributes(&fa, kern);
+    if (e != cudaSuccess) return cuda_fail(e, "kernel shared-memory attributes");
+    e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, optin - (int)fa.sharedSizeBytes);
     if (e != cudaSuccess) return cuda_fail(e, "cudaFuncSetAttribute");
     info.configured = true;
     info.blocks_per_sm = 0;
@@ -1353,10 +1784,14 @@ int launch_gather(KArgs k, cudaStream_t stream) {
   static LaunchInfo info;
   static std::mutex mu;
   using TabT = typename MapTraits<MapT>::Tab;
-  const int tab_cap = (HAS_QU && k.ring_table != nullptr) ? table_slots<TabT, min_blocks<MODE, MapT>()>(k.tab_req) : 0;
-  const size_t smem = kTabHeaderBytes + sizeof(TabT) * (size_t)tab_cap;
+  constexpr int MINB = min_blocks<MODE, MapT>();
+  const int tab_cap = (HAS_QU && k.ring_table != nullptr) ? table_slots<TabT, MINB>(k.tab_req) : 0;
+  const size_t tab_end = kTabHeaderBytes + align16(sizeof(TabT) * (size_t)tab_cap);
+  const size_t stage = beam_stage_bytes(k.S, PM == kParamsRef32 ? sizeof(float) : sizeof(double));
+  k.beam_stage = (k.flags_stage && tab_end + stage <= cta_smem_budget<MINB>()) ? 1 : 0;
+  const size_t smem = tab_end + (k.beam_stage ? stage : 0);
   int blocks_per_sm = 0;
-  const int rc = configure_launch<TabT, min_blocks<MODE, MapT>()>(kern, info, mu, smem, blocks_per_sm);
+  const int rc = configure_launch<TabT, MINB>(kern, info, mu, smem, blocks_per_sm);
   if (rc != TODGPU_OK) return rc;
   k.tab_cap = tab_cap;
   const long long max_blocks = (long long)sm_count() * blocks_per_sm;
@@ -1384,12 +1819,25 @@ int launch_batched(BatchParams& bp, bool any_table, cudaStream_t stream) {
     req = std::max(req, bp.job[j].tab_req);
     any_default = any_default || bp.job[j].tab_req == 0;
   }
-  const int tab_cap = (HAS_QU && any_table) ? table_slots<TabT, min_blocks<MODE, MapT>()>(any_default ? 0 : req) : 0;
-  const size_t smem = kTabHeaderBytes + sizeof(TabT) * (size_t)tab_cap;
+  constexpr int MINB = min_blocks<MODE, MapT>();
+  const int tab_cap = (HAS_QU && any_table) ? table_slots<TabT, MINB>(any_default ? 0 : req) : 0;
+  const size_t tab_end = kTabHeaderBytes + align16(sizeof(TabT) * (size_t)tab_cap);
+  // one shared region for every job's beam: sized for the largest
+  size_t stage = 0;
+  bool want_stage = true;
+  for (int j = 0; j < bp.njobs; ++j) {
+    stage = std::max(stage, beam_stage_bytes(bp.job[j].S, PM == kParamsRef32 ? sizeof(float) : sizeof(double)));
+    want_stage = want_stage && bp.job[j].flags_stage;
+  }
+  const int staged = (want_stage && tab_end + stage <= cta_smem_budget<MINB>()) ? 1 : 0;
+  const size_t smem = tab_end + (staged ? stage : 0);
   int blocks_per_sm = 0;
-  const int rc = configure_launch<TabT, min_blocks<MODE, MapT>()>(kern, info, mu, smem, blocks_per_sm);
+  const int rc = configure_launch<TabT, MINB>(kern, info, mu, smem, blocks_per_sm);
   if (rc != TODGPU_OK) return rc;
-  for (int j = 0; j < bp.njobs; ++j) bp.job[j].tab_cap = tab_cap;
+  for (int j = 0; j < bp.njobs; ++j) {
+    bp.job[j].tab_cap = tab_cap;
+    bp.job[j].beam_stage = staged;
+  }
   const long long T = bp.tiles_before[bp.njobs];
   if (T == 0) return TODGPU_OK;
   const long long max_blocks = (long long)sm_count() * blocks_per_sm;
@@ -1419,9 +1867,7 @@ int dispatch_qu(const KArgs& k, bool has_qu, cudaStream_t s) {
 template <int MODE, typename MapT>
 int dispatch_single_pm(const KArgs& k, bool has_qu, int params_dtype, cudaStream_t s) {
   if (params_dtype == TODGPU_F32) return dispatch_qu<MODE, MapT, kParamsRef32>(k, has_qu, s);
-  if (params_dtype == TODGPU_F64)
-    return k.S >= kShareRotMinS ? dispatch_qu<MODE, MapT, kParamsF64Shared>(k, has_qu, s)
-                                : dispatch_qu<MODE, MapT, kParamsF64>(k, has_qu, s);
+  if (params_dtype == TODGPU_F64) return dispatch_qu<MODE, MapT, kParamsF64>(k, has_qu, s);
   return dispatch_qu<MODE, MapT, kAngles>(k, has_qu, s);
 }
 

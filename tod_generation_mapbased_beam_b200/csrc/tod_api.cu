@@ -38,7 +38,8 @@ __global__ void ring_table_kernel(long long nside, double reach, RingRec* t, boo
       }
     }
     r.cap = cap;
-    r.pre = 0;
+    r.unused = 0;
+    r.first32 = (int)ri.first;
     r.inv_dphi = 1.0 / ri.dphi;
     r.inv_dta = ir < nrings ? 1.0 / (acos(hp_ring_z(nside, ir + 1)) - r.ta) : 0.0;
     t[ir] = r;
@@ -53,37 +54,11 @@ __global__ void ring_table_kernel(long long nside, double reach, RingRec* t, boo
     h.first = 0;
     h.n = 0;
     h.cap = 0;
-    h.pre = 0;
+    h.first32 = 0;
+    h.unused = 0;
     h.inv_dphi = 0.0;
     h.inv_dta = 0.0;
     t[0] = h;
-  }
-}
-
-// Exclusive prefix sum of cap over rings 1..nrings into `pre` (one CTA of
-// 1024 threads: per-thread chunk sums, a block scan, then the chunks).
-__global__ void ring_prefix_kernel(long long nside, RingRec* t) {
-  __shared__ long long part[1024];
-  const long long nrings = 4 * nside - 1;
-  const long long chunk = (nrings + blockDim.x - 1) / blockDim.x;
-  const long long lo = 1 + threadIdx.x * chunk, hi = min(nrings + 1, lo + chunk);
-  long long sum = 0;
-  for (long long ir = lo; ir < hi; ++ir) sum += t[ir].cap;
-  part[threadIdx.x] = sum;
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    long long run = 0;
-    for (int i = 0; i < (int)blockDim.x; ++i) {
-      const long long v = part[i];
-      part[i] = run;
-      run += v;
-    }
-  }
-  __syncthreads();
-  long long run = part[threadIdx.x];
-  for (long long ir = lo; ir < hi; ++ir) {
-    t[ir].pre = run;
-    run += t[ir].cap;
   }
 }
 
@@ -269,7 +244,8 @@ __global__ void __launch_bounds__(kNTStatic) static_reach_kernel(const KArgs a, 
     h.first = 0;
     h.n = 0;
     h.cap = 0;
-    h.pre = 0;
+    h.first32 = 0;
+    h.unused = 0;
     h.inv_dphi = 0.0;
     h.inv_dta = 0.0;
     t[0] = h;
@@ -360,10 +336,14 @@ static int check_common(const todgpu_gather_args* a, bool need_map) {
   if (a->nside < 1 || a->nside > kMaxNside)
     return fail(TODGPU_ENSIDE, "nside " + std::to_string(a->nside) + " outside [1, 16384]");
   if (a->B < 0 || a->S < 0) return fail(TODGPU_ESHAPE, "negative B or S");
+  if (a->S > (1LL << 29)) return fail(TODGPU_ESHAPE, "S above 2^29 beam pixels");
   if (a->tab_slots < 0) return fail(TODGPU_EINVAL, "tab_slots must be >= 0");
   if (a->params_dtype != TODGPU_F32 && a->params_dtype != TODGPU_F64 && a->params_dtype != TODGPU_ANGLES)
     return fail(TODGPU_EDTYPE, "params_dtype must be TODGPU_F32, TODGPU_F64 or TODGPU_ANGLES");
   if (a->B > 0 && a->S > 0) {
+    const uintptr_t vec_align = a->params_dtype == TODGPU_F32 ? 3 : 7;
+    if (((uintptr_t)a->vec_orig & vec_align) != 0 || ((uintptr_t)a->beam_vals & 3) != 0)
+      return fail(TODGPU_EINVAL, "vec_orig and beam_vals must be aligned to their element size");
     if (a->params_dtype == TODGPU_ANGLES) {
       if (!a->vec_orig || !a->theta || !a->phi || !a->psi) return fail(TODGPU_EINVAL, "NULL pointing array");
       if (a->angles_dtype != TODGPU_F32 && a->angles_dtype != TODGPU_F64)
@@ -436,6 +416,8 @@ static KArgs make_kargs(const todgpu_gather_args* a) {
   if (k.ring_table != nullptr && (((uintptr_t)k.ring_table & 15) != 0)) k.ring_table = nullptr;
   k.tab_cap = 0;
   k.tab_req = a->tab_slots;
+  k.flags_stage = (a->flags & TODGPU_FLAG_NO_BEAM_STAGE) ? 0 : 1;
+  k.beam_stage = 0;
   return k;
 }
 
@@ -493,17 +475,16 @@ extern "C" int todgpu_gather_accum_static(const todgpu_gather_args* a, void* str
   cudaStream_t s = static_cast<cudaStream_t>(stream);
   const bool has_qu = (a->c_q >= 0 && a->c_u >= 0);
   if (!(a->flags & TODGPU_FLAG_NO_TABLES)) {
-    // every call rebuilds the whole table (header, records, prefix sums) for
-    // its own nside and beam, so nothing depends on earlier contents.  Without
-    // Q and U the gather reads only the ring records (no spin-2 tables): the
-    // header then carries a zero reach and the slot sums are not built.
+    // every call rebuilds the whole table (header and records) for its own
+    // nside and beam, so nothing depends on earlier contents.  Without Q and U
+    // the gather reads only the ring records (no spin-2 tables): the header
+    // then carries a zero reach.
     if (has_qu) {
       if (a->params_dtype == TODGPU_F32)
         static_reach_kernel<kParamsRef32><<<1, kNTStatic, 0, s>>>(k, t);
       else
         static_reach_kernel<kParamsF64><<<1, kNTStatic, 0, s>>>(k, t);
       ring_table_kernel<<<grid_for(4 * a->nside, 256), 256, 0, s>>>(a->nside, 0.0, t, true);
-      ring_prefix_kernel<<<1, 1024, 0, s>>>(a->nside, t);
     } else {
       ring_table_kernel<<<grid_for(4 * a->nside, 256), 256, 0, s>>>(a->nside, 0.0, t, false);
     }
@@ -514,6 +495,12 @@ extern "C" int todgpu_gather_accum_static(const todgpu_gather_args* a, void* str
     k.ring_table = nullptr;
   }
   return dispatch_types(k, a->interp, has_qu, a->map_dtype, a->params_dtype, s);
+}
+
+extern "C" int64_t todgpu_gather_wait_timeouts(void) {
+  unsigned long long v = 0;
+  if (cudaMemcpyFromSymbol(&v, g_gather_wait_timeouts, sizeof(v)) != cudaSuccess) return -1;
+  return (int64_t)v;
 }
 
 extern "C" int todgpu_gather_accum_batched(const todgpu_gather_args* jobs, int32_t njobs, int64_t tile,
@@ -661,7 +648,6 @@ extern "C" int todgpu_ring_table_build(int64_t nside, double reach, void* table,
   cudaStream_t s = static_cast<cudaStream_t>(stream);
   RingRec* t = static_cast<RingRec*>(table);
   ring_table_kernel<<<grid_for(4 * nside, 256), 256, 0, s>>>(nside, reach, t, false);
-  ring_prefix_kernel<<<1, 1024, 0, s>>>(nside, t);
   cudaError_t e = cudaGetLastError();
   return e == cudaSuccess ? TODGPU_OK : cuda_fail(e, "ring table kernels");
 }

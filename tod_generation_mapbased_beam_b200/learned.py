@@ -114,25 +114,50 @@ class LearnedTailTOD:
 
     # -- the network -----------------------------------------------------------
     def fit(self, n_train=1 << 18, steps=4000, batch=8192, seed=6, net=None, lr_max=2e-3, lr_min=2e-5,
-            **net_kwargs):
+            group=None, **net_kwargs):
         """Tail targets at ``n_train`` uniform pointings (plain method), then
-        training.  Returns timing and loss information."""
+        training.  Returns timing and loss information.
+
+        ``group``: a torch.distributed process group (one process per GPU, all
+        calling fit with the same arguments).  Each rank then computes the
+        targets of its share of the pointings and the ranks train together
+        (``dp_train.DataParallelTrainer``: gradients all-reduced every step,
+        ``batch`` rows per step over all ranks); every rank ends with the same
+        network."""
+        import torch.distributed as dist
+
+        world = dist.get_world_size(group) if (group is not None or dist.is_initialized()) else 1
+        rank = dist.get_rank(group) if world > 1 else 0
         t0 = time.perf_counter()
         th, ph, ps = uniform_pointings(int(n_train), seed)
+        if world > 1:
+            from .sharding import sample_shard
+
+            a, b = sample_shard(int(n_train), rank, world)
+            th, ph, ps = th[a:b], ph[a:b], ps[a:b]
         th_d, ph_d, ps_d = (torch.from_numpy(a).to(self.device) for a in (th, ph, ps))
         target = self.plain_tail(th_d, ph_d, ps_d)
         torch.cuda.synchronize()
         t1 = time.perf_counter()
         self.net = net if net is not None else TailNet(n_out=3, **net_kwargs)
         x = self.net.inputs(th_d, ph_d, ps_d)
-        losses = self.net.fit(x[:th.size], target.T.contiguous(), steps=steps, batch=batch, lr_max=lr_max,
-                              lr_min=lr_min)
+        if world > 1:
+            from .dp_train import DataParallelTrainer
+
+            trainer = DataParallelTrainer(self.net, group)
+            trainer.sync_parameters()
+            losses = trainer.fit(x[:th.size], target.T.contiguous(), steps, batch // world, lr_max=lr_max,
+                                 lr_min=lr_min)
+        else:
+            losses = self.net.fit(x[:th.size], target.T.contiguous(), steps=steps, batch=batch, lr_max=lr_max,
+                                  lr_min=lr_min)
         torch.cuda.synchronize()
         t2 = time.perf_counter()
         self.judged = None
         return dict(n_train=int(n_train), steps=int(steps), batch=int(batch), target_seconds=t1 - t0,
                     train_seconds=t2 - t1, loss_first=float(losses[:10].mean()),
-                    loss_last=float(losses[-100:].mean()), target_rms_K=target.std(dim=1).cpu().numpy().tolist())
+                    loss_last=float(losses[-100:].mean()), target_rms_K=target.std(dim=1).cpu().numpy().tolist(),
+                    ranks=world)
 
     def learned_tail(self, theta, phi, psi, tod=None):
         """Tail contribution from the network, (3, B) float64."""

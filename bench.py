@@ -86,6 +86,9 @@ def parse_args():
     p.add_argument("--learned-train", type=int, default=1 << 18,
                    help="training pointings of the learned tail (plain-method targets)")
     p.add_argument("--learned-steps", type=int, default=4000, help="training steps of the learned tail")
+    p.add_argument("--learned-curve", type=str, default=None,
+                   help="comma-separated training-set sizes: print the learned tail's held-out error per size "
+                        "(targets of the largest, nested subsets) instead of the benchmark")
     p.add_argument("--no-tables", action="store_true",
                    help="evaluate ring data and spin-2 angles directly (A/B comparison)")
     p.add_argument("--no-beam-stage", action="store_true",
@@ -795,6 +798,47 @@ def run_learned(args, dist, sky):
     }
 
 
+def run_learned_curve(args, sizes):
+    """Held-out error of the learned tail (config 5) against the training-set
+    size: plain-method targets at max(sizes) uniform pointings (seed 6), a
+    network trained on each nested prefix (same steps and batch), judged on
+    4096 samples of the config-2 scan against the plain float64 path."""
+    import torch
+
+    from tod_generation_mapbased_beam_b200 import learned as L
+    from tod_generation_mapbased_beam_b200 import sky as SKY
+    from tod_generation_mapbased_beam_b200 import workloads as W
+    from tod_generation_mapbased_beam_b200.tailnet import TailNet
+
+    dev = torch.device("cuda")
+    sky = SKY.synfast_iqu(2048, seed=2)
+    main, tail = W.config5_beams()
+    lt = L.LearnedTailTOD(2048, sky, main, tail)
+    n_max = max(sizes)
+    t0 = time.perf_counter()
+    th, ph, ps = L.uniform_pointings(n_max, 6)
+    ang = [torch.from_numpy(a).to(dev) for a in (th, ph, ps)]
+    target = lt.plain_tail(*ang)
+    torch.cuda.synchronize()
+    target_s = time.perf_counter() - t0
+    B = args.samples
+    sth, sph, sps = W.spin_scan(B, 100.0)
+    idx = np.linspace(0, B - 1, 4096).astype(np.int64)
+    held = [torch.from_numpy(a[idx].copy()).to(dev) for a in (sth, sph, sps)]
+    out = []
+    for n in sorted(sizes):
+        lt.net = TailNet(n_out=3)
+        x = lt.net.inputs(*[a[:n] for a in ang])
+        t1 = time.perf_counter()
+        losses = lt.net.fit(x[:n], target[:, :n].T.contiguous(), steps=args.learned_steps, batch=8192)
+        torch.cuda.synchronize()
+        j = lt.judge(*held, budget_uK=0.1)
+        out.append({"n_train": n, "err_rms_uK": g4(j["learned"]["rms_uK"]), "err_max_uK": g4(j["learned"]["max_uK"]),
+                    "loss_last": g4(float(losses[-100:].mean())), "train_s": g4(time.perf_counter() - t1)})
+    return {"curve": out, "dropped_rms_uK": g4(j["dropped"]["rms_uK"]), "target_s": g4(target_s),
+            "targets": n_max, "steps": args.learned_steps, "held_out": 4096}
+
+
 # ---------------------------------------------------------------------------
 # the CPU arm
 # ---------------------------------------------------------------------------
@@ -837,6 +881,10 @@ def main():
         print(json.dumps(line))
         return
 
+    if args.learned_curve:
+        print(json.dumps(run_learned_curve(args, [int(v) for v in args.learned_curve.split(",")]),
+                         separators=(",", ":")))
+        return
     dist = Dist()
     res, B, S = run_ours(args, dist)
     if not (args.no_learned and args.no_precision and args.no_batched):

@@ -253,7 +253,7 @@ def test_data_parallel_trainer_on_one_rank_equals_fused_training():
     ph = rng.uniform(0, 2 * np.pi, n)
     ps = rng.uniform(0, 2 * np.pi, n)
     target = np.stack([np.sin(2 * th) * np.cos(ph), np.cos(ps) * th, np.sin(ph + ps)], -1) * 1e-7
-    nets = [TailNet(n_freq=32, width=128, depth=2, n_out=3, seed=4) for _ in range(2)]
+    nets = [TailNet(n_freq=64, width=128, depth=2, n_out=3, seed=4) for _ in range(2)]
     x = nets[0].inputs(th, ph, ps)
     fused = nets[0].fit(x, target, steps=40, batch=512)
     dp = DataParallelTrainer(nets[1]).fit(x, target, 40, 512)

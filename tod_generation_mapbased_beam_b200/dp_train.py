@@ -35,9 +35,13 @@ __all__ = ["DataParallelTrainer", "cosine_lr"]
 
 
 def cosine_lr(step, total_steps, lr_max, lr_min):
-    """Learning rate of step ``step`` (0-based), as todgpu_mlp_train sets it."""
+    """Learning rate of step ``step`` (0-based), as todgpu_mlp_train sets it:
+    float32 lr_max and lr_min and their float32 difference, the cosine factor
+    in float64, the result rounded to float32."""
+    hi, lo = np.float32(lr_max), np.float32(lr_min)
+    span = float(np.float32(hi - lo))
     c = 0.5 * (1.0 + math.cos(math.pi * float(step) / float(max(1, total_steps))))
-    return float(np.float32(lr_min + (lr_max - lr_min) * c))
+    return float(np.float32(float(lo) + span * c))
 
 
 class DataParallelTrainer:

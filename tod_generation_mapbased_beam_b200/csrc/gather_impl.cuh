@@ -1658,7 +1658,10 @@ __global__ void __launch_bounds__(NT, MINB) gather_accum_kernel(const KArgs a) {
 // neighbouring samples of one job (the same sky region, shared in L2), and
 // every CTA gets an equal share of every job whatever its beam size.  `tile`
 // sets how many consecutive samples a CTA takes at a time.  The descriptors
-// travel in the kernel parameters.
+// travel in the kernel parameters; each CTA copies the current job's into
+// shared memory, so that the sample loop reads its fields with plain shared
+// loads rather than parameter loads at a job index known only at run time
+// (5% of the batched launch).
 constexpr int kMaxBatchJobs = 96;
 struct BatchParams {
   int njobs;
@@ -1671,13 +1674,20 @@ template <int MODE, bool HAS_QU, typename MapT, int PM, int LAYOUT, int NT, int 
 __global__ void __launch_bounds__(NT, MINB) gather_batched_kernel(const __grid_constant__ BatchParams p) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   __shared__ double s_red[(NT / 32) * 4];
+  __shared__ __align__(16) KArgs s_job;
   const long long G = gridDim.x, k = blockIdx.x;
   for (int j = 0; j < p.njobs; ++j) {
     const long long ntiles = p.tiles_before[j + 1] - p.tiles_before[j];
     // first tile of job j that falls to this CTA: global index = k (mod G)
     const long long t0 = ((k - p.tiles_before[j]) % G + G) % G;
-    if (t0 < ntiles)
-      run_samples<MODE, HAS_QU, MapT, PM, LAYOUT, NT>(p.job[j], t0, ntiles, G, p.tile, smem_raw, s_red);
+    if (t0 < ntiles) {
+      __syncthreads();
+      if (threadIdx.x < (int)(sizeof(KArgs) / 8))
+        reinterpret_cast<unsigned long long*>(&s_job)[threadIdx.x] =
+            reinterpret_cast<const unsigned long long*>(&p.job[j])[threadIdx.x];
+      __syncthreads();
+      run_samples<MODE, HAS_QU, MapT, PM, LAYOUT, NT>(s_job, t0, ntiles, G, p.tile, smem_raw, s_red);
+    }
   }
 }
 
@@ -1803,6 +1813,7 @@ int launch_gather(KArgs k, cudaStream_t stream) {
 }
 
 static_assert(sizeof(BatchParams) <= 32000, "batched descriptors must fit the kernel parameter space");
+static_assert(sizeof(KArgs) % 8 == 0 && sizeof(KArgs) / 8 <= 256, "KArgs copied as 8-byte words");
 
 // Batched launch: descriptors of up to kMaxBatchJobs jobs per launch.
 template <int MODE, bool HAS_QU, typename MapT, int PM, int LAYOUT>

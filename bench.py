@@ -241,10 +241,10 @@ def make_workload(n_samples, rank, gpu_sky=True):
 
 
 def bench_config(args, S, world):
-    return {"workload": f"config2 plain FP64 {args.mode}: nside 1024 f64 I/Q/U sky (f64 records), 30' beam "
-                        f"@ nside 2048 0.99 cut, 100 Hz spin scan, one I/Q/U entry (spin-2)",
+    return {"workload": f"config2 FP64 {args.mode}: nside 1024 IQU sky, 30' beam @2048 0.99 cut, 100 Hz scan, "
+                        "spin-2",
             "samples_per_gpu": args.samples, "S": S, "mode": args.mode,
-            "l2": "inputs > L2 (~1 GB), no flush", "params": "reference float32 rotation parameters",
+            "l2": "inputs > L2, no flush", "params": "reference f32",
             "parallelism": f"samples x{world}"}
 
 
@@ -465,9 +465,11 @@ def run_ours(args, dist):
 
     def step():
         tods[args.mode].zero_()
+        torch.cuda.nvtx.range_push("plain_step")
         k0.record(stream)
         launch(args.mode)
         k1.record(stream)
+        torch.cuda.nvtx.range_pop()
 
     for _ in range(args.warmup):
         step()
@@ -508,11 +510,10 @@ def run_ours(args, dist):
     roofline = {"bound": "l2", "achieved": g4(g_gbs), "peak": g4(l2_peak), "unit": "GB/s", "frac": g4(g_frac),
                 "traffic": None, "kernel": "gather_accum_kernel", "kernel_ms": g4(kernel_ms),
                 "bytes_per_sample": S * STENCIL[args.mode] * 32,
-                "peak_source": "todgpu_l2_probe, measured in this run",
-                "ref_equiv_fp64_tflops": g4(ref_tflops), "fp64_peak_tflops": g4(fp64_peak),
+                "peak_source": "todgpu_l2_probe, this run",
+                "fp64_peak_tflops": g4(fp64_peak),
                 "ref_equiv_fp64_frac": g4(ref_tflops / fp64_peak),
-                "hbm_frac": g4(hbm_bytes / (kernel_ms / 1e3) / 1e9 / peaks["hbm_gbs"]),
-                "hbm_peak_source": peak_src}
+                "hbm_frac": g4(hbm_bytes / (kernel_ms / 1e3) / 1e9 / peaks["hbm_gbs"])}
     result = {"value": value, "ms_per_step": total_ms / args.steps, "roofline": roofline, "clocks": clk,
               "gpu_launches": args.steps}
 
@@ -536,7 +537,7 @@ def run_ours(args, dist):
         nthreads = len(os.sched_getaffinity(0))
         n_sub = min(args.parity_samples, B)
         idx = np.unique(np.linspace(0, B - 1, n_sub).astype(np.int64))
-        par = {"samples": int(idx.size), "of": B, "spread": "evenly over the day"}
+        par = {"samples": int(idx.size)}
         idx_d = to(idx)
         for m in modes:
             rel = oracle_parity(wl, params_h, order, tods[m][:, idx_d].cpu().numpy(), m, idx, nthreads)
@@ -615,7 +616,7 @@ def run_ours(args, dist):
         assert day.shape == (3, B)
         result["e2e"] = {"value": B * dist.world * args.steps / e2e_s, "unit": "samples/s",
                          "h2d_bytes_per_step": int(B * 3 * 4), "d2h_bytes_per_step": int(B * 3 * 8),
-                         "api": "driver.DayRunner.run: host f32 (theta, phi, psi) -> host f64 tod_day (3, n)"}
+                         "api": "DayRunner.run, host angles -> host f64 TOD"}
         drop_s, res = timed(lambda: tod_core.beam_tod_batch(nside, None, data, wl["rot"], wl["phi"],
                                                             wl["theta"], wl["psis"],
                                                             interp_mode=args.mode))
@@ -626,8 +627,7 @@ def run_ours(args, dist):
     if not args.no_cpu_baseline and dist.rank == 0:
         rate, n, threads = cpu_rate(wl, args.mode, args.cpu_seconds)
         result["cpu_baseline"] = {"value": g4(rate), "unit": "samples/s", "cores": threads, "kind": "port",
-                                  "sample": f"{n} consecutive samples (S={S}, nside {nside}), C/OpenMP oracle, "
-                                            "best of 2"}
+                                  "sample": f"{n} consecutive samples, C/OpenMP oracle, best of 2"}
     return result, B, S
 
 
@@ -677,7 +677,7 @@ def run_precision(args, dist, sky):
         subs[kind] = tod[:, idx_d].cpu().numpy()
         rec = {"f64": 32, "f32": 16, "bf16": 8}[kind]
         _, fr = gather_frac(B, beam.S, args.mode, rec, ms, l2_peak)
-        out[kind] = {"value": g4(B * dist.world / (ms / 1e3)), "ms": g4(ms), "gather_frac": g4(fr)}
+        out[kind] = {"value": g4(B * dist.world / (ms / 1e3)), "gather_frac": g4(fr)}
         del tod, mp
     if dist.rank == 0 and not args.no_cpu_baseline:
         t0 = time.perf_counter()
@@ -691,8 +691,7 @@ def run_precision(args, dist, sky):
         oracle_s = time.perf_counter() - t0
     else:
         oracle_s = None
-    return {"S": beam.S, "forms": out, "error_vs": f"FP64 CPU oracle, {n_sub} samples spread over the day",
-            "oracle_seconds": g4(oracle_s)}
+    return {"S": beam.S, "forms": out, "err_vs": f"FP64 oracle, {n_sub} samples"}
 
 
 def run_batched(args, dist, sky):
@@ -730,7 +729,7 @@ def run_batched(args, dist, sky):
     loop_ms = dist.max(statistics.mean(_evt_ms(loop, stream) for _ in range(2)))
     batch.release()
     return {"value": g4(n * dist.world / (ms / 1e3)), "ms": g4(ms), "samples": n, "tile": batch.tile,
-            "per_detector_value": g4(n * dist.world / (loop_ms / 1e3)), "autotune_s": g4(tune_s)}
+            "per_detector_value": g4(n * dist.world / (loop_ms / 1e3))}
 
 
 def run_learned(args, dist, sky):
@@ -763,11 +762,13 @@ def run_learned(args, dist, sky):
     main_ms, net_ms = [], []
     for i in range(args.warmup + args.steps):
         tod.zero_()
+        torch.cuda.nvtx.range_push("learned_form")
         ev[0].record(stream)
         lt.main_lobe(*scan, tod)
         ev[1].record(stream)
         lt.learned_tail(*scan, tod)
         ev[2].record(stream)
+        torch.cuda.nvtx.range_pop()
         ev[2].synchronize()
         if i >= args.warmup:
             main_ms.append(ev[0].elapsed_time(ev[1]))
@@ -789,12 +790,12 @@ def run_learned(args, dist, sky):
         "value": g4(value), "ms": g4(step_ms), "plain_fp64_value": g4(plain_rate),
         "speedup_vs_plain_fp64": g4(value / (plain_rate * dist.world)),
         "err_rms_uK": g4(judged["learned"]["rms_uK"]), "dropped_rms_uK": g4(judged["dropped"]["rms_uK"]),
-        "err_max_uK": g4(judged["learned"]["max_uK"]), "budget_uK": 0.1,
+        "budget_uK": 0.1,
         "within_budget_per_component": bool(judged["use_surrogate"]),
         "dropped_within_budget": bool(max(judged["dropped"]["rms_uK"]) <= 0.1),
         "main_ms": g4(statistics.mean(main_ms)), "net_ms": g4(net_ms_mean),
         "net_tflops": g4(net_tflops), "net_frac_bf16_sustained": g4(net_tflops / peak),
-        "n_train": info["n_train"], "target_s": g4(info["target_seconds"]), "train_s": g4(info["train_seconds"]),
+        "n_train": info["n_train"],
     }
 
 
@@ -863,8 +864,8 @@ def main():
     args = parse_args()
     base = {"metric": METRIC, "unit": "samples/s", "higher_is_better": True, "steps": args.steps,
             "warmup": args.warmup, "vs_baseline": None, "dtype": "f64",
-            "data": "synthetic: seeded 100 Hz spin scan, pole-centred Gaussian beam, seeded synfast-like "
-                    "I/Q/U sky (GPU alm2map; the CPU arm a seeded Gaussian sky of the same RMS)"}
+            "data": "synthetic: seeded spin scan, Gaussian beam, synfast-like I/Q/U sky (GPU; CPU arm: Gaussian "
+                    "sky, same RMS)"}
     if args.impl == "reference":
         r = run_reference(args)
         if r is None:

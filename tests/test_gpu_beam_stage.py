@@ -5,8 +5,9 @@ beam (pixel vectors and weights) into shared memory with bulk copies and the
 pixel loop reads it from there; the 16-byte aligned middle of each array goes
 by cp.async.bulk, the unaligned ends by plain loads.  The TOD must be the same
 bit for bit as with the beam read from global memory (TODGPU_FLAG_NO_BEAM_STAGE),
-for every pointing mode, both interpolation modes, beams whose arrays start
-at any element offset, and beams too large to stage (read from global memory
+for every pointing mode, both interpolation modes (nearest launches never
+stage: the comparison then covers the flag alone), beams whose arrays start at
+any element offset, and beams too large to stage (read from global memory
 either way).  No bounded wait of the copies may run out."""
 
 import numpy as np

@@ -1428,9 +1428,9 @@ static __device__ __noinline__ void footprint_window(const KArgs& a, const RingR
   // for any footprint of that reach.  Away from the poles the disc's
   // half-width in longitude on a ring at colatitude theta_r is
   // sqrt(reach^2 - (theta_r - theta_u)^2) / sin theta_r to within a
-  // percent for reach < 0.05; 5% margin and one pixel either side keep
-  // every stencil pixel in.  (A pixel outside its ring's slots is still
-  // evaluated, directly; only the cost changes.)
+  // percent for reach < 0.05; 2% margin and the rounding up of the
+  // half-width keep every stencil pixel in.  (A pixel outside its ring's
+  // slots is still evaluated, directly; only the cost changes.)
   const bool disc = reach < 0.05 && theta_u - reach > 0.1 && theta_u + reach < kPi - 0.1;
   if (fits) {
     for (int t = threadIdx.x; t < nr; t += kSetupThreads) {
@@ -1440,8 +1440,8 @@ static __device__ __noinline__ void footprint_window(const KArgs& a, const RingR
       if (disc) {
         const double dth = __ldg(&r->ta) - theta_u;
         const double h2 = reach * reach - dth * dth;
-        const int k = h2 > 0.0 ? (int)ceil(1.05 * sqrt(h2) / __ldg(&r->sth) * __ldg(&r->inv_dphi)) : 0;
-        cnt = min(cnt, 2 * k + 3);
+        const int k = h2 > 0.0 ? (int)ceil(1.02 * sqrt(h2) / __ldg(&r->sth) * __ldg(&r->inv_dphi)) : 0;
+        cnt = min(cnt, 2 * k + 1);
       }
       int iplo = 0;
       if (cnt < n) {
@@ -1511,10 +1511,12 @@ __device__ void run_samples(const KArgs& a, long long t_begin, long long t_end, 
     beam_extent<PM, NT>(a, s_red, cx, cy, cz, rbeam);
     // every stencil neighbour centre lies within 1.7/nside rad of the query
     // (one ring spacing plus one pixel width; the opposite pair around a pole
-    // within twice the colatitude of ring 1); 3/nside leaves margin, plus
+    // within twice the colatitude of ring 1); 2/nside leaves margin, plus
     // slack for the float32 parameter rounding.  A neighbour outside the
-    // window is still evaluated correctly (directly), only slower.
-    reach = rbeam + 3.0 / (double)a.nside + 1e-5;
+    // window is still evaluated correctly (directly), only slower (measured:
+    // 3/nside and 5% more slots per ring made the tables ~25% larger and
+    // config 2 ~3% slower).
+    reach = rbeam + 2.0 / (double)a.nside + 1e-5;
     // the ring table reserves per-ring slots for footprints up to its reach
     use_tab = reach <= __ldg(&rt[0].ta);
   }
@@ -1747,6 +1749,14 @@ constexpr int max_table_slots() {
 }
 constexpr size_t align16(size_t x) { return (x + 15) & ~size_t(15); }
 
+// Modes whose launches stage the beam in shared memory when it fits: bilinear
+// (config 2: +5%); nearest reads one stencil pixel per beam pixel and gains
+// more from the shared memory left to L1 (config 2: 1% faster without).
+template <int MODE>
+constexpr bool stage_beam_mode() {
+  return MODE == TODGPU_BILINEAR;
+}
+
 // Dynamic shared memory a CTA may take while MINB CTAs still fit on an SM.
 template <int MINB>
 constexpr size_t cta_smem_budget() {
@@ -1798,7 +1808,7 @@ int launch_gather(KArgs k, cudaStream_t stream) {
   const int tab_cap = (HAS_QU && k.ring_table != nullptr) ? table_slots<TabT, MINB>(k.tab_req) : 0;
   const size_t tab_end = kTabHeaderBytes + align16(sizeof(TabT) * (size_t)tab_cap);
   const size_t stage = beam_stage_bytes(k.S, PM == kParamsRef32 ? sizeof(float) : sizeof(double));
-  k.beam_stage = (k.flags_stage && tab_end + stage <= cta_smem_budget<MINB>()) ? 1 : 0;
+  k.beam_stage = (stage_beam_mode<MODE>() && k.flags_stage && tab_end + stage <= cta_smem_budget<MINB>()) ? 1 : 0;
   const size_t smem = tab_end + (k.beam_stage ? stage : 0);
   int blocks_per_sm = 0;
   const int rc = configure_launch<TabT, MINB>(kern, info, mu, smem, blocks_per_sm);
@@ -1840,7 +1850,7 @@ int launch_batched(BatchParams& bp, bool any_table, cudaStream_t stream) {
     stage = std::max(stage, beam_stage_bytes(bp.job[j].S, PM == kParamsRef32 ? sizeof(float) : sizeof(double)));
     want_stage = want_stage && bp.job[j].flags_stage;
   }
-  const int staged = (want_stage && tab_end + stage <= cta_smem_budget<MINB>()) ? 1 : 0;
+  const int staged = (stage_beam_mode<MODE>() && want_stage && tab_end + stage <= cta_smem_budget<MINB>()) ? 1 : 0;
   const size_t smem = tab_end + (staged ? stage : 0);
   int blocks_per_sm = 0;
   const int rc = configure_launch<TabT, MINB>(kern, info, mu, smem, blocks_per_sm);

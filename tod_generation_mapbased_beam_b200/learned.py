@@ -126,7 +126,7 @@ class LearnedTailTOD:
         network."""
         import torch.distributed as dist
 
-        world = dist.get_world_size(group) if (group is not None or dist.is_initialized()) else 1
+        world = dist.get_world_size(group) if group is not None else 1
         rank = dist.get_rank(group) if world > 1 else 0
         t0 = time.perf_counter()
         th, ph, ps = uniform_pointings(int(n_train), seed)

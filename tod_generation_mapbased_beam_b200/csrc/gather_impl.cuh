@@ -1372,14 +1372,239 @@ __device__ __noinline__ Contrib bilinear_full(const KArgs& a, const SampleBlock*
   return out;
 }
 
-template <int MODE, bool HAS_QU, typename MapT, int LAYOUT, typename TabT, class Acc>
-__device__ __forceinline__ void eval_fast(const KArgs& a, const SampleBlock* sb, const RingRec* rt,
-                                          const Spin2Tab& w, const TabT* tab, double vx, double vy, double vz,
-                                          double phi_w, float bvf, Acc& acc) {
+// The nearest rule's full path (poles and their neighbourhood, candidates
+// more than 0.02 rad apart in longitude, near-ties, neighbours outside the
+// spin-2 table), out of line, returning its terms by value.
+template <bool HAS_QU, typename MapT, int LAYOUT, typename TabT>
+__device__ __noinline__ Contrib nearest_full(const KArgs& a, const SampleBlock* sb, const RingRec* rt,
+                                             const Spin2Tab& w, const TabT* tab, int2 hdr, double vx, double vy,
+                                             double vz, double phi_w, float bvf) {
   constexpr bool kPacked = MapTraits<MapT>::packed;
   const Chan<LAYOUT> ch(a);
   const int nside = (int)a.nside;
   const double bv = (double)bvf;
+  Contrib out{{0.0, 0.0, 0.0, 0.0}, 0};
+  // nearest: unclamped z; |z| > 1 makes the reference's ring_above NaN-based
+  // and the clamp then picks ring 1 (numba_healpy.py:62-70, tod_nearest.py:115-120)
+  const double sin_th = sqrt(max0(vx * vx + vy * vy));
+  int ir_above;
+  if (fabs(vz) <= 1.0) {
+    ir_above = ring_above_fast(nside, vz);
+    ir_above = ir_above < 1 ? 1 : (ir_above > 4 * nside - 2 ? 4 * nside - 2 : ir_above);
+  } else {
+    ir_above = 1;
+  }
+  // The four candidates: two pixels on each of rings ir_above and
+  // ir_above + 1, ranked by the cosine of their angular distance.  A first
+  // pass evaluates cos(phi_w - phic) by cos_small where the difference is at
+  // most kCosSmallMax (cos() beyond); the two differ by < 2e-15, so a lead of more
+  // than 1e-13 over the runner-up picks the pixel that ranking by cos()
+  // picks.  A closer call is ranked again by cos() itself -- the same
+  // expression, order and strict comparison -- so the pixel is always the
+  // one of ranking by cos() throughout.
+  int best_g = -1, best_ip = 0;
+  const RingNear rg0 = ring_near(rt, ir_above), rg1 = ring_near(rt, ir_above + 1);
+  {
+    double lead = -3.0, runner = -3.0;
+#pragma unroll
+    for (int g = 0; g < 2; ++g) {
+      const RingNear& r = g == 0 ? rg0 : rg1;
+      int ipb = (int)div_rn(phi_w * (double)r.n, kTwoPi, kInvTwoPi);
+      if (ipb >= r.n) ipb -= r.n;
+#pragma unroll
+      for (int t = 0; t < 2; ++t) {
+        const int ip = (t == 0) ? ipb : wrap_up(ipb, 1, r.n);
+        const double dl = phi_w - (r.phi0 + (double)ip * r.dphi);
+        const double cosd = sin_th * r.sth * (fabs(dl) <= kCosSmallMax ? cos_small(dl) : cos(dl)) + vz * r.z;
+        if (cosd > lead) {
+          runner = lead;
+          lead = cosd;
+          best_g = g;
+          best_ip = ip;
+        } else if (cosd > runner) {
+          runner = cosd;
+        }
+      }
+    }
+    if (!(lead - runner > 1e-13)) {
+      double best_cos = -2.0;
+      best_g = -1;
+#pragma unroll
+      for (int g = 0; g < 2; ++g) {
+        const RingNear& r = g == 0 ? rg0 : rg1;
+        int ipb = (int)(phi_w * (double)r.n / kTwoPi);
+        if (ipb >= r.n) ipb -= r.n;
+#pragma unroll
+        for (int t = 0; t < 2; ++t) {
+          const int ip = (t == 0) ? ipb : wrap_up(ipb, 1, r.n);
+          const double phic = r.phi0 + (double)ip * r.dphi;
+          const double cosd = sin_th * r.sth * cos(phi_w - phic) + vz * r.z;
+          if (cosd > best_cos) {
+            best_cos = cosd;
+            best_g = g;
+            best_ip = ip;
+          }
+        }
+      }
+    }
+  }
+  int best_pix = 0, best_n = 1, best_ring = 0;
+  double best_zc = 0.0, best_phic = 0.0;
+  if (best_g >= 0) {
+    const RingNear& r = best_g == 0 ? rg0 : rg1;
+    best_ring = ir_above + best_g;
+    best_n = r.n;
+    best_pix = r.first + best_ip;
+    best_zc = r.z;
+    best_phic = r.phi0 + (double)best_ip * r.dphi;
+  } else {
+    best_ip = 0;
+  }
+  RingWin rw{0, 0, 0, false};
+  if constexpr (HAS_QU) rw = ring_win(w, hdr, best_ring);
+  if constexpr (kPacked) {
+    const float4 rec = load_rec<MapT>(a, best_pix);
+    float c2f = 1.f, s2f = 0.f;
+    if constexpr (HAS_QU) {
+      double c2d, s2d;
+      spin2_win(rw, tab, sb, best_ip, best_n, best_zc, best_phic, c2d, s2d);
+      c2f = (float)c2d;
+      s2f = (float)s2d;
+    }
+#pragma unroll
+    for (int c = 0; c < 4; ++c) {
+      if (c >= ch.C) break;
+      if (HAS_QU && c == ch.q)
+        out.v[c] = (double)(fmaf(rec_at(rec, ch.q), c2f, rec_at(rec, ch.u) * s2f) * bvf);
+      else if (HAS_QU && c == ch.u)
+        out.v[c] = (double)(fmaf(rec_at(rec, ch.u), c2f, -rec_at(rec, ch.q) * s2f) * bvf);
+      else
+        out.v[c] = (double)(rec_at(rec, c) * bvf);
+    }
+  } else if constexpr (HAS_QU) {
+    double c2d, s2d;
+    spin2_win(rw, tab, sb, best_ip, best_n, best_zc, best_phic, c2d, s2d);
+    const double qv = map_i<MapT>(a, ch.q, best_pix);
+    const double uv = map_i<MapT>(a, ch.u, best_pix);
+#pragma unroll
+    for (int c = 0; c < 4; ++c) {
+      if (c >= ch.C) break;
+      if (c == ch.q)
+        out.v[c] = (double)(fma(qv, c2d, uv * s2d) * bv);
+      else if (c == ch.u)
+        out.v[c] = (double)(fma(uv, c2d, -qv * s2d) * bv);
+      else
+        out.v[c] = (double)(map_x_beam_i<MapT>(a, c, best_pix, bvf));
+    }
+  } else {
+#pragma unroll
+    for (int c = 0; c < 4; ++c) {
+      if (c >= ch.C) break;
+      out.v[c] = (double)(map_x_beam_i<MapT>(a, c, best_pix, bvf));
+    }
+  }
+  return out;
+}
+
+// The nearest rule in the common case, without branches: a query within the
+// rings of the map (|z| <= 1), all four candidates within kCosSmallMax of it in
+// longitude (so ranked by cos_small), a lead over the runner-up above 1e-13
+// (so no re-ranking by cos()), and with Q and U the chosen pixel in the
+// sample's spin-2 table.  The same operations on the same values as the full
+// path; returns false (having added nothing) when any of these does not hold.
+template <bool HAS_QU, typename MapT, int LAYOUT, typename TabT, class Acc>
+__device__ __forceinline__ bool nearest_lean(const KArgs& a, const RingRec* rt, const Spin2Tab& w, const TabT* tab,
+                                             const int2& hdr, double vx, double vy, double vz, double phi_w,
+                                             float bvf, Acc& acc) {
+  constexpr bool kPacked = MapTraits<MapT>::packed;
+  const int nside = (int)a.nside;
+  if (!(fabs(vz) <= 1.0)) return false;
+  const double sin_th = sqrt(max0(vx * vx + vy * vy));
+  int ir_above = ring_above_fast(nside, vz);
+  ir_above = ir_above < 1 ? 1 : (ir_above > 4 * nside - 2 ? 4 * nside - 2 : ir_above);
+  const RingNear rg0 = ring_near(rt, ir_above), rg1 = ring_near(rt, ir_above + 1);
+  int best_g = -1, best_ip = 0;
+  double lead = -3.0, runner = -3.0;
+  bool small = true;
+#pragma unroll
+  for (int g = 0; g < 2; ++g) {
+    const RingNear& r = g == 0 ? rg0 : rg1;
+    int ipb = (int)div_rn(phi_w * (double)r.n, kTwoPi, kInvTwoPi);
+    if (ipb >= r.n) ipb -= r.n;
+#pragma unroll
+    for (int t = 0; t < 2; ++t) {
+      const int ip = (t == 0) ? ipb : wrap_up(ipb, 1, r.n);
+      const double dl = phi_w - (r.phi0 + (double)ip * r.dphi);
+      small = small && fabs(dl) <= kCosSmallMax;
+      const double cosd = sin_th * r.sth * cos_small(dl) + vz * r.z;
+      if (cosd > lead) {
+        runner = lead;
+        lead = cosd;
+        best_g = g;
+        best_ip = ip;
+      } else if (cosd > runner) {
+        runner = cosd;
+      }
+    }
+  }
+  if (!(small && lead - runner > 1e-13 && best_g >= 0)) return false;
+  const RingNear& r = best_g == 0 ? rg0 : rg1;
+  const int best_pix = r.first + best_ip;
+  double c2d = 1.0, s2d = 0.0;
+  if constexpr (HAS_QU) {
+    const RingWin rw = ring_win(w, hdr, ir_above + best_g);
+    int j = best_ip - rw.iplo;
+    j += (j >> 31) & r.n;
+    if (!(rw.in && (unsigned)j < (unsigned)rw.cap)) return false;
+    const TabT v = tab[rw.off + j];
+    c2d = (double)v.x;
+    s2d = (double)v.y;
+  }
+  const Chan<LAYOUT> ch(a);
+  if constexpr (kPacked) {
+    const float4 rec = load_rec<MapT>(a, best_pix);
+    const float c2f = (float)c2d, s2f = (float)s2d;
+#pragma unroll
+    for (int c = 0; c < 4; ++c) {
+      if (c >= ch.C) break;
+      if (HAS_QU && c == ch.q)
+        acc.add(c, fmaf(rec_at(rec, ch.q), c2f, rec_at(rec, ch.u) * s2f) * bvf);
+      else if (HAS_QU && c == ch.u)
+        acc.add(c, fmaf(rec_at(rec, ch.u), c2f, -rec_at(rec, ch.q) * s2f) * bvf);
+      else
+        acc.add(c, rec_at(rec, c) * bvf);
+    }
+  } else if constexpr (HAS_QU) {
+    const double bv = (double)bvf;
+    const double qv = map_i<MapT>(a, ch.q, best_pix);
+    const double uv = map_i<MapT>(a, ch.u, best_pix);
+#pragma unroll
+    for (int c = 0; c < 4; ++c) {
+      if (c >= ch.C) break;
+      if (c == ch.q)
+        acc.add(c, fma(qv, c2d, uv * s2d) * bv);
+      else if (c == ch.u)
+        acc.add(c, fma(uv, c2d, -qv * s2d) * bv);
+      else
+        acc.add(c, map_x_beam_i<MapT>(a, c, best_pix, bvf));
+    }
+  } else {
+#pragma unroll
+    for (int c = 0; c < 4; ++c) {
+      if (c >= ch.C) break;
+      acc.add(c, map_x_beam_i<MapT>(a, c, best_pix, bvf));
+    }
+  }
+  return true;
+}
+
+// One beam pixel on the fast path: the branch-free common case of its mode,
+// else that mode's full path out of line.
+template <int MODE, bool HAS_QU, typename MapT, int LAYOUT, typename TabT, class Acc>
+__device__ __forceinline__ void eval_fast(const KArgs& a, const SampleBlock* sb, const RingRec* rt,
+                                          const Spin2Tab& w, const TabT* tab, double vx, double vy, double vz,
+                                          double phi_w, float bvf, Acc& acc) {
+  const Chan<LAYOUT> ch(a);
   int2 hdr = make_int2(0, 0);  // {first window ring, window rings}
   if constexpr (HAS_QU) hdr = lds_i2(&w.hdr);
   if constexpr (MODE == TODGPU_BILINEAR) {
@@ -1393,123 +1618,12 @@ __device__ __forceinline__ void eval_fast(const KArgs& a, const SampleBlock* sb,
       }
     }
   } else {
-    // nearest: unclamped z; |z| > 1 makes the reference's ring_above NaN-based
-    // and the clamp then picks ring 1 (numba_healpy.py:62-70, tod_nearest.py:115-120)
-    const double sin_th = sqrt(max0(vx * vx + vy * vy));
-    int ir_above;
-    if (fabs(vz) <= 1.0) {
-      ir_above = ring_above_fast(nside, vz);
-      ir_above = ir_above < 1 ? 1 : (ir_above > 4 * nside - 2 ? 4 * nside - 2 : ir_above);
-    } else {
-      ir_above = 1;
-    }
-    // The four candidates: two pixels on each of rings ir_above and
-    // ir_above + 1, ranked by the cosine of their angular distance.  A first
-    // pass evaluates cos(phi_w - phic) by cos_small where the difference is at
-    // most kCosSmallMax (cos() beyond); the two differ by < 2e-15, so a lead of more
-    // than 1e-13 over the runner-up picks the pixel that ranking by cos()
-    // picks.  A closer call is ranked again by cos() itself -- the same
-    // expression, order and strict comparison -- so the pixel is always the
-    // one of ranking by cos() throughout.
-    int best_g = -1, best_ip = 0;
-    const RingNear rg0 = ring_near(rt, ir_above), rg1 = ring_near(rt, ir_above + 1);
-    {
-      double lead = -3.0, runner = -3.0;
-#pragma unroll
-      for (int g = 0; g < 2; ++g) {
-        const RingNear& r = g == 0 ? rg0 : rg1;
-        int ipb = (int)div_rn(phi_w * (double)r.n, kTwoPi, kInvTwoPi);
-        if (ipb >= r.n) ipb -= r.n;
-#pragma unroll
-        for (int t = 0; t < 2; ++t) {
-          const int ip = (t == 0) ? ipb : wrap_up(ipb, 1, r.n);
-          const double dl = phi_w - (r.phi0 + (double)ip * r.dphi);
-          const double cosd = sin_th * r.sth * (fabs(dl) <= kCosSmallMax ? cos_small(dl) : cos(dl)) + vz * r.z;
-          if (cosd > lead) {
-            runner = lead;
-            lead = cosd;
-            best_g = g;
-            best_ip = ip;
-          } else if (cosd > runner) {
-            runner = cosd;
-          }
-        }
-      }
-      if (!(lead - runner > 1e-13)) {
-        double best_cos = -2.0;
-        best_g = -1;
-#pragma unroll
-        for (int g = 0; g < 2; ++g) {
-          const RingNear& r = g == 0 ? rg0 : rg1;
-          int ipb = (int)(phi_w * (double)r.n / kTwoPi);
-          if (ipb >= r.n) ipb -= r.n;
-#pragma unroll
-          for (int t = 0; t < 2; ++t) {
-            const int ip = (t == 0) ? ipb : wrap_up(ipb, 1, r.n);
-            const double phic = r.phi0 + (double)ip * r.dphi;
-            const double cosd = sin_th * r.sth * cos(phi_w - phic) + vz * r.z;
-            if (cosd > best_cos) {
-              best_cos = cosd;
-              best_g = g;
-              best_ip = ip;
-            }
-          }
-        }
-      }
-    }
-    int best_pix = 0, best_n = 1, best_ring = 0;
-    double best_zc = 0.0, best_phic = 0.0;
-    if (best_g >= 0) {
-      const RingNear& r = best_g == 0 ? rg0 : rg1;
-      best_ring = ir_above + best_g;
-      best_n = r.n;
-      best_pix = r.first + best_ip;
-      best_zc = r.z;
-      best_phic = r.phi0 + (double)best_ip * r.dphi;
-    } else {
-      best_ip = 0;
-    }
-    RingWin rw{0, 0, 0, false};
-    if constexpr (HAS_QU) rw = ring_win(w, hdr, best_ring);
-    if constexpr (kPacked) {
-      const float4 rec = load_rec<MapT>(a, best_pix);
-      float c2f = 1.f, s2f = 0.f;
-      if constexpr (HAS_QU) {
-        double c2d, s2d;
-        spin2_win(rw, tab, sb, best_ip, best_n, best_zc, best_phic, c2d, s2d);
-        c2f = (float)c2d;
-        s2f = (float)s2d;
-      }
+    if (!nearest_lean<HAS_QU, MapT, LAYOUT>(a, rt, w, tab, hdr, vx, vy, vz, phi_w, bvf, acc)) {
+      const Contrib r = nearest_full<HAS_QU, MapT, LAYOUT>(a, sb, rt, w, tab, hdr, vx, vy, vz, phi_w, bvf);
 #pragma unroll
       for (int c = 0; c < 4; ++c) {
         if (c >= ch.C) break;
-        if (HAS_QU && c == ch.q)
-          acc.add(c, fmaf(rec_at(rec, ch.q), c2f, rec_at(rec, ch.u) * s2f) * bvf);
-        else if (HAS_QU && c == ch.u)
-          acc.add(c, fmaf(rec_at(rec, ch.u), c2f, -rec_at(rec, ch.q) * s2f) * bvf);
-        else
-          acc.add(c, rec_at(rec, c) * bvf);
-      }
-    } else if constexpr (HAS_QU) {
-      double c2d, s2d;
-      spin2_win(rw, tab, sb, best_ip, best_n, best_zc, best_phic, c2d, s2d);
-      const double qv = map_i<MapT>(a, ch.q, best_pix);
-      const double uv = map_i<MapT>(a, ch.u, best_pix);
-#pragma unroll
-      for (int c = 0; c < 4; ++c) {
-        if (c >= ch.C) break;
-        if (c == ch.q)
-          acc.add(c, fma(qv, c2d, uv * s2d) * bv);
-        else if (c == ch.u)
-          acc.add(c, fma(uv, c2d, -qv * s2d) * bv);
-        else
-          acc.add(c, map_x_beam_i<MapT>(a, c, best_pix, bvf));
-      }
-    } else {
-#pragma unroll
-      for (int c = 0; c < 4; ++c) {
-        if (c >= ch.C) break;
-        acc.add(c, map_x_beam_i<MapT>(a, c, best_pix, bvf));
+        acc.add(c, r.v[c]);
       }
     }
   }

@@ -1599,10 +1599,7 @@ __device__ __forceinline__ bool nearest_lean(const KArgs& a, const RingRec* rt, 
 }
 
 // One beam pixel on the fast path: the branch-free common case of its mode,
-// else that mode's full path out of line.  With Q and U but no spin-2 table
-// for the sample (a footprint larger than the table or the ring table's
-// reach: hdr.y == 0, the same for the whole CTA) the common case cannot
-// hold, so the full path runs without trying it.
+// else that mode's full path out of line.
 template <int MODE, bool HAS_QU, typename MapT, int LAYOUT, typename TabT, class Acc>
 __device__ __forceinline__ void eval_fast(const KArgs& a, const SampleBlock* sb, const RingRec* rt,
                                           const Spin2Tab& w, const TabT* tab, double vx, double vy, double vz,
@@ -1610,10 +1607,9 @@ __device__ __forceinline__ void eval_fast(const KArgs& a, const SampleBlock* sb,
   const Chan<LAYOUT> ch(a);
   int2 hdr = make_int2(0, 0);  // {first window ring, window rings}
   if constexpr (HAS_QU) hdr = lds_i2(&w.hdr);
-  const bool try_lean = !HAS_QU || hdr.y != 0;
   if constexpr (MODE == TODGPU_BILINEAR) {
     const double z = clamp1(vz);
-    if (!(try_lean && bilinear_lean<HAS_QU, MapT, LAYOUT>(a, rt, w, tab, hdr, z, phi_w, bvf, acc))) {
+    if (!bilinear_lean<HAS_QU, MapT, LAYOUT>(a, rt, w, tab, hdr, z, phi_w, bvf, acc)) {
       const Contrib r = bilinear_full<HAS_QU, MapT, LAYOUT>(a, sb, rt, w, tab, hdr, z, phi_w, bvf);
 #pragma unroll
       for (int c = 0; c < 4; ++c) {
@@ -1622,7 +1618,7 @@ __device__ __forceinline__ void eval_fast(const KArgs& a, const SampleBlock* sb,
       }
     }
   } else {
-    if (!(try_lean && nearest_lean<HAS_QU, MapT, LAYOUT>(a, rt, w, tab, hdr, vx, vy, vz, phi_w, bvf, acc))) {
+    if (!nearest_lean<HAS_QU, MapT, LAYOUT>(a, rt, w, tab, hdr, vx, vy, vz, phi_w, bvf, acc)) {
       const Contrib r = nearest_full<HAS_QU, MapT, LAYOUT>(a, sb, rt, w, tab, hdr, vx, vy, vz, phi_w, bvf);
 #pragma unroll
       for (int c = 0; c < 4; ++c) {

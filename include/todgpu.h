@@ -40,6 +40,9 @@ extern "C" {
                                    angle directly (same results, slower) */
 #define TODGPU_FLAG_NO_BEAM_STAGE 2 /* read the beam from global memory even when the launch
                                        could hold it in shared memory (same results) */
+#define TODGPU_FLAG_WIDE_CTAS 4 /* launch 256-thread CTAs even where the spin-2 table asked
+                                   for (tab_slots) fits 128-thread CTAs at 8 per SM
+                                   (same results) */
 
 /* Element types. */
 #define TODGPU_F32 0

@@ -22,6 +22,7 @@ F32, F64, ANGLES = 0, 1, 2
 PACKED_F32, PACKED_BF16, PACKED_F64 = 2, 3, 4
 FLAG_NO_TABLES = 1
 FLAG_NO_BEAM_STAGE = 2
+FLAG_WIDE_CTAS = 4
 
 _i32 = ctypes.c_int32
 _i64 = ctypes.c_int64

@@ -30,7 +30,7 @@ from .kernels import (_map_tensor, _ncomp, _row_stride, _set_map, beam_order, be
 
 class DetectorBatch:
     def __init__(self, nside, mp, detectors, comp_indices=(0, 1, 2), interp_mode="bilinear",
-                 tile=None, graph=True, tables=True, precompute=True):
+                 tile=None, graph=True, tables=True, precompute=True, wide_ctas=False):
         require_cuda()
         if interp_mode not in ("bilinear", "nearest"):
             raise ValueError(f"interp_mode {interp_mode!r} not available on main branch; "
@@ -65,7 +65,9 @@ class DetectorBatch:
             reach = beam_reach(vec, self.nside) if (tables and vec.shape[0]) else 0.0
             self.tables.append(ring_table(self.nside, reach, dev) if reach > 0 else None)
         self.rot = [pointing_buffers(a[0].shape[0], dev) for a in self.angles] if precompute else None
-        self.flags = 0 if tables else _native.FLAG_NO_TABLES
+        # wide_ctas: 256-thread CTAs even where the tables fit 128-thread ones
+        # (same TOD; for timing and tests)
+        self.flags = (0 if tables else _native.FLAG_NO_TABLES) | (_native.FLAG_WIDE_CTAS if wide_ctas else 0)
         self._args = self._make_args()
         self.tile = int(tile) if tile else None
         self.use_graph = graph

@@ -3,8 +3,10 @@
 // instantiate them (gather_map_*.cu, one per map element type) and by the C
 // ABI (tod_api.cu).
 //
-// Work decomposition ("footprint" kernel): a persistent grid of 256-thread
-// CTAs walks the samples; a CTA takes one sample at a time and
+// Work decomposition ("footprint" kernel): a persistent grid of CTAs (128
+// threads, 8 per SM, when the sample's spin-2 table fits an eighth of an SM's
+// shared memory; else 256 threads, 3-4 per SM) walks the samples; a CTA takes
+// one sample at a time and
 //   1. rotates the beam's centre direction with the sample's rotation to get
 //      the footprint centre, and derives the window of RING rings the
 //      footprint (beam radius + stencil reach) can touch;
@@ -17,8 +19,9 @@
 //   4. strides its threads over the beam pixels: rotate -> atan2/clamp ->
 //      RING stencil (ring data from the window) -> spin-2 (from the table) ->
 //      gather -> FP64 accumulate;
-//   5. reduces the per-thread sums in a fixed order and adds them into
-//      tod[c, b] (one writer per sample: no atomics, bit-reproducible runs).
+//   5. reduces the per-lane sums (256 summation lanes in either CTA shape) in
+//      a fixed order and adds them into tod[c, b] (one writer per sample: no
+//      atomics, bit-reproducible runs, the same TOD in both shapes).
 // Table values are produced by the same functions on the same inputs as
 // direct evaluation, so they are bit-identical to it; any lookup outside the
 // window (or a footprint too large for the tables) falls back to direct
@@ -50,6 +53,11 @@ constexpr int kRingCap = 192;   // rings per footprint window
 constexpr int kTabCapDefault = 2048;  // spin-2 table slots per sample (32 KB)
 constexpr long long kMaxNside = 16384;
 constexpr int kNTStatic = 256;  // threads of the reach kernel of the built-in table
+// Summation lanes of the gather: the beam pixels of a sample are summed in
+// kSumLanes strided partial sums (then per warp of lanes, then over those in
+// order), whatever the CTA's thread count, so CTAs of 128 and 256 threads
+// give the same TOD bit for bit.
+constexpr int kSumLanes = 256;
 
 // Message of the calling thread's last failure (defined in tod_api.cu).
 extern thread_local std::string g_last_error;
@@ -91,6 +99,8 @@ struct KArgs {
   unsigned long long* err;
   int flags_stage;           // the caller allows staging the beam in shared memory
   int beam_stage;            // the launch made room for the beam in shared memory
+  int flags_wide;            // the caller asks for 256-thread CTAs
+  int unused;
 };
 
 // Pointing modes of the per-sample rotation.
@@ -1728,6 +1738,7 @@ template <int MODE, bool HAS_QU, typename MapT, int PM, int LAYOUT, int NT>
 __device__ void run_samples(const KArgs& a, long long t_begin, long long t_end, long long t_step, long long tile,
                             unsigned char* smem_raw, double* s_red) {
   constexpr int NW = NT / 32;
+  static_assert(NT >= 2 * kSetupThreads && kSumLanes % NT == 0, "CTA of 128 or 256 threads");
   Spin2Tab& w = *reinterpret_cast<Spin2Tab*>(smem_raw);
   using TabT = typename MapTraits<MapT>::Tab;
   using Acc = typename std::conditional<MapTraits<MapT>::packed, AccKahan, Acc64>::type;
@@ -1791,7 +1802,7 @@ __device__ void run_samples(const KArgs& a, long long t_begin, long long t_end, 
     }
     const bool has_next = tn < t_end && bn < a.B;
     if (warp == kRotWarp && has_next) prefetch_fields<PM>(a, bn, s_raw, lane);
-    if (prev >= 0 && threadIdx.x == 0) flush_sample<NW>(a, s_red, prev);
+    if (prev >= 0 && threadIdx.x == 0) flush_sample<kSumLanes / 32>(a, s_red, prev);
     if (use_tab) {
       if (threadIdx.x < kSetupThreads) {
         // footprint window of this sample (same values in every setup thread)
@@ -1825,52 +1836,60 @@ __device__ void run_samples(const KArgs& a, long long t_begin, long long t_end, 
     }
     __syncthreads();
 
-    Acc acc;
-    for (int s = threadIdx.x; s < S; s += NT) {
-      VecT v0, v1, v2;
-      float bvf;
-      if (staged) {
-        v0 = svec[3 * s];
-        v1 = svec[3 * s + 1];
-        v2 = svec[3 * s + 2];
-        bvf = sbv[s];
-      } else {
-        const VecT* v = static_cast<const VecT*>(a.vec) + 3 * s;
-        v0 = __ldg(v);
-        v1 = __ldg(v + 1);
-        v2 = __ldg(v + 2);
-        bvf = __ldg(a.beam + s);
-      }
-      double vx, vy, vz;
-      rotate_block(sb, v0, v1, v2, vx, vy, vz);
-      double phi_w = atan2(vy, vx);
-      if (phi_w < 0.0) phi_w += kTwoPi;
-      if (fast && isfinite(vx) && isfinite(vy) && isfinite(vz)) {
-        eval_fast<MODE, HAS_QU, MapT, LAYOUT>(a, sb, rt, w, tab, vx, vy, vz, phi_w, bvf, acc);
-      } else if constexpr (MODE == TODGPU_BILINEAR) {
-        const Contrib r = rt != nullptr
-                              ? eval_generic<MODE, HAS_QU, MapT>(a, sb, TableRings{rt}, w, tab, vx, vy, vz, phi_w, bvf)
-                              : eval_generic<MODE, HAS_QU, MapT>(a, sb, DirectRings{a.nside, a.npix}, w, tab, vx, vy,
-                                                                 vz, phi_w, bvf);
-        if (r.err) {
-          ++nerr;
+    // summation lane l (of kSumLanes) takes the beam pixels l, l + kSumLanes,
+    // ...; thread t is lane t + i NT in pass i, so the TOD does not depend on
+    // the CTA's thread count
+#pragma unroll 1
+    for (int pass = 0; pass < kSumLanes / NT; ++pass) {
+      const int sl = threadIdx.x + pass * NT;
+      Acc acc;
+      for (int s = sl; s < S; s += kSumLanes) {
+        VecT v0, v1, v2;
+        float bvf;
+        if (staged) {
+          v0 = svec[3 * s];
+          v1 = svec[3 * s + 1];
+          v2 = svec[3 * s + 2];
+          bvf = sbv[s];
         } else {
-#pragma unroll
-          for (int c = 0; c < 4; ++c)
-            if (c < a.C) acc.add(c, r.v[c]);
+          const VecT* v = static_cast<const VecT*>(a.vec) + 3 * s;
+          v0 = __ldg(v);
+          v1 = __ldg(v + 1);
+          v2 = __ldg(v + 2);
+          bvf = __ldg(a.beam + s);
         }
-      } else if (rt != nullptr) {
-        eval_generic_into<MODE, HAS_QU, MapT>(a, sb, TableRings{rt}, w, tab, vx, vy, vz, phi_w, bvf, acc, nerr);
-      } else {
-        eval_generic_into<MODE, HAS_QU, MapT>(a, sb, DirectRings{a.nside, a.npix}, w, tab, vx, vy, vz, phi_w, bvf,
-                                              acc, nerr);
-      }
-    }
+        double vx, vy, vz;
+        rotate_block(sb, v0, v1, v2, vx, vy, vz);
+        double phi_w = atan2(vy, vx);
+        if (phi_w < 0.0) phi_w += kTwoPi;
+        if (fast && isfinite(vx) && isfinite(vy) && isfinite(vz)) {
+          eval_fast<MODE, HAS_QU, MapT, LAYOUT>(a, sb, rt, w, tab, vx, vy, vz, phi_w, bvf, acc);
+        } else if constexpr (MODE == TODGPU_BILINEAR) {
+          const Contrib r =
+              rt != nullptr
+                  ? eval_generic<MODE, HAS_QU, MapT>(a, sb, TableRings{rt}, w, tab, vx, vy, vz, phi_w, bvf)
+                  : eval_generic<MODE, HAS_QU, MapT>(a, sb, DirectRings{a.nside, a.npix}, w, tab, vx, vy, vz, phi_w,
+                                                     bvf);
+          if (r.err) {
+            ++nerr;
+          } else {
 #pragma unroll
-    for (int c = 0; c < 4; ++c) {
-      if (c >= a.C) break;
-      const double v = warp_sum(acc.total(c));
-      if (lane == 0) s_red[warp * 4 + c] = v;
+            for (int c = 0; c < 4; ++c)
+              if (c < a.C) acc.add(c, r.v[c]);
+          }
+        } else if (rt != nullptr) {
+          eval_generic_into<MODE, HAS_QU, MapT>(a, sb, TableRings{rt}, w, tab, vx, vy, vz, phi_w, bvf, acc, nerr);
+        } else {
+          eval_generic_into<MODE, HAS_QU, MapT>(a, sb, DirectRings{a.nside, a.npix}, w, tab, vx, vy, vz, phi_w, bvf,
+                                                acc, nerr);
+        }
+      }
+#pragma unroll
+      for (int c = 0; c < 4; ++c) {
+        if (c >= a.C) break;
+        const double v = warp_sum(acc.total(c));
+        if (lane == 0) s_red[(sl >> 5) * 4 + c] = v;
+      }
     }
     // the next sample's rotation into the other block (read after the next barrier)
     if (warp == kRotWarp && has_next) {
@@ -1882,7 +1901,7 @@ __device__ void run_samples(const KArgs& a, long long t_begin, long long t_end, 
     prev = b;
   }
   __syncthreads();
-  if (prev >= 0 && threadIdx.x == 0) flush_sample<NW>(a, s_red, prev);
+  if (prev >= 0 && threadIdx.x == 0) flush_sample<kSumLanes / 32>(a, s_red, prev);
   if (a.err != nullptr) {
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) nerr += __shfl_xor_sync(0xffffffffu, nerr, o);
@@ -1894,7 +1913,7 @@ __device__ void run_samples(const KArgs& a, long long t_begin, long long t_end, 
 template <int MODE, bool HAS_QU, typename MapT, int PM, int LAYOUT, int NT, int MINB>
 __global__ void __launch_bounds__(NT, MINB) gather_accum_kernel(const KArgs a) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  __shared__ double s_red[(NT / 32) * 4];
+  __shared__ double s_red[(kSumLanes / 32) * 4];
   run_samples<MODE, HAS_QU, MapT, PM, LAYOUT, NT>(a, blockIdx.x, a.B, gridDim.x, 1, smem_raw, s_red);
 }
 
@@ -1922,7 +1941,7 @@ struct BatchParams {
 template <int MODE, bool HAS_QU, typename MapT, int PM, int LAYOUT, int NT, int MINB>
 __global__ void __launch_bounds__(NT, MINB) gather_batched_kernel(const __grid_constant__ BatchParams p) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  __shared__ double s_red[(NT / 32) * 4];
+  __shared__ double s_red[(kSumLanes / 32) * 4];
   __shared__ __align__(16) KArgs s_job;
   const long long G = gridDim.x, k = blockIdx.x;
   for (int j = 0; j < p.njobs; ++j) {
@@ -2018,7 +2037,7 @@ int table_slots(int requested) {
 
 // Once per kernel: allow the largest table; per launch: CTAs per SM for the
 // launch's shared memory (recomputed when it changes).
-template <typename TabT, int MINB, typename Kern>
+template <int NT, typename Kern>
 int configure_launch(Kern kern, LaunchInfo& info, std::mutex& mu, size_t smem, int& blocks_per_sm) {
   std::lock_guard<std::mutex> lock(mu);
   if (!info.configured) {
@@ -2036,7 +2055,7 @@ int configure_launch(Kern kern, LaunchInfo& info, std::mutex& mu, size_t smem, i
   }
   if (info.blocks_per_sm == 0 || info.smem != smem) {
     int nb = 0;
-    cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, kern, kNT, smem);
+    cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, kern, NT, smem);
     if (e != cudaSuccess) return cuda_fail(e, "cudaOccupancyMaxActiveBlocksPerMultiprocessor");
     info.blocks_per_sm = std::max(nb, 1);
     info.smem = smem;
@@ -2045,49 +2064,68 @@ int configure_launch(Kern kern, LaunchInfo& info, std::mutex& mu, size_t smem, i
   return TODGPU_OK;
 }
 
-template <int MODE, bool HAS_QU, typename MapT, int PM, int LAYOUT>
-int launch_gather(KArgs k, cudaStream_t stream) {
-  auto kern = gather_accum_kernel<MODE, HAS_QU, MapT, PM, LAYOUT, kNT, min_blocks<MODE, MapT>()>;
+// Two CTA shapes.  Wide: kNT (256) threads, min_blocks() CTAs per SM, room
+// for the default 32 KiB spin-2 table and the staged beam.  Narrow: 128
+// threads, 8 CTAs per SM at 64 registers, for launches whose requested table
+// fits an eighth of an SM's shared memory (config 2: 1.1k slots of 16 B): with
+// twice the CTAs per SM, the per-sample setup and barriers of one CTA overlap
+// the pixel loops of more others (config 2 bilinear +12%, nearest +7%, although
+// the beam no longer fits beside the table).  Larger footprints (config 3:
+// 3.3k slots) keep the wide shape: in the narrow one their tables would not fit
+// and their samples would fall back to direct spin-2 evaluation.  The TOD is
+// the same bit for bit in either shape (kSumLanes).
+constexpr int kNTNarrow = 128;
+constexpr int kMinbNarrow = 8;
+
+template <typename TabT>
+constexpr bool narrow_fits(int requested) {
+  return requested > 0 && requested <= max_table_slots<TabT, kMinbNarrow>();
+}
+
+template <int MODE, bool HAS_QU, typename MapT, int PM, int LAYOUT, int NT, int MINB>
+int launch_gather_shape(KArgs k, cudaStream_t stream) {
+  auto kern = gather_accum_kernel<MODE, HAS_QU, MapT, PM, LAYOUT, NT, MINB>;
   static LaunchInfo info;
   static std::mutex mu;
   using TabT = typename MapTraits<MapT>::Tab;
-  constexpr int MINB = min_blocks<MODE, MapT>();
   const int tab_cap = (HAS_QU && k.ring_table != nullptr) ? table_slots<TabT, MINB>(k.tab_req) : 0;
   const size_t tab_end = kTabHeaderBytes + align16(sizeof(TabT) * (size_t)tab_cap);
   const size_t stage = beam_stage_bytes(k.S, PM == kParamsRef32 ? sizeof(float) : sizeof(double));
   k.beam_stage = (stage_beam_mode<MODE>() && k.flags_stage && tab_end + stage <= cta_smem_budget<MINB>()) ? 1 : 0;
   const size_t smem = tab_end + (k.beam_stage ? stage : 0);
   int blocks_per_sm = 0;
-  const int rc = configure_launch<TabT, MINB>(kern, info, mu, smem, blocks_per_sm);
+  const int rc = configure_launch<NT>(kern, info, mu, smem, blocks_per_sm);
   if (rc != TODGPU_OK) return rc;
   k.tab_cap = tab_cap;
   const long long max_blocks = (long long)sm_count() * blocks_per_sm;
   const int grid = (int)std::max(1LL, std::min(k.B, max_blocks));
-  kern<<<grid, kNT, smem, stream>>>(k);
+  kern<<<grid, NT, smem, stream>>>(k);
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return cuda_fail(e, "gather_accum_kernel launch");
   return TODGPU_OK;
 }
 
-static_assert(sizeof(BatchParams) <= 32000, "batched descriptors must fit the kernel parameter space");
-static_assert(sizeof(KArgs) % 8 == 0 && sizeof(KArgs) / 8 <= 256, "KArgs copied as 8-byte words");
-
-// Batched launch: descriptors of up to kMaxBatchJobs jobs per launch.
 template <int MODE, bool HAS_QU, typename MapT, int PM, int LAYOUT>
-int launch_batched(BatchParams& bp, bool any_table, cudaStream_t stream) {
-  auto kern = gather_batched_kernel<MODE, HAS_QU, MapT, PM, LAYOUT, kNT, min_blocks<MODE, MapT>()>;
+int launch_gather(KArgs k, cudaStream_t stream) {
+  using TabT = typename MapTraits<MapT>::Tab;
+  if (!k.flags_wide && narrow_fits<TabT>(k.tab_req))
+    return launch_gather_shape<MODE, HAS_QU, MapT, PM, LAYOUT, kNTNarrow, kMinbNarrow>(k, stream);
+  return launch_gather_shape<MODE, HAS_QU, MapT, PM, LAYOUT, kNT, min_blocks<MODE, MapT>()>(k, stream);
+}
+
+static_assert(sizeof(BatchParams) <= 32000, "batched descriptors must fit the kernel parameter space");
+static_assert(sizeof(KArgs) % 8 == 0 && sizeof(KArgs) / 8 <= kNTNarrow, "KArgs copied as 8-byte words, one per thread");
+
+// Batched launch: descriptors of up to kMaxBatchJobs jobs per launch, in one
+// CTA shape: narrow when every job allows it and the table size the launch
+// takes (the largest any job asks for; a job asking for the default makes it
+// the default) fits it.
+template <int MODE, bool HAS_QU, typename MapT, int PM, int LAYOUT, int NT, int MINB>
+int launch_batched_shape(BatchParams& bp, bool any_table, int req, bool any_default, cudaStream_t stream) {
+  auto kern = gather_batched_kernel<MODE, HAS_QU, MapT, PM, LAYOUT, NT, MINB>;
   static LaunchInfo info;
   static std::mutex mu;
   using TabT = typename MapTraits<MapT>::Tab;
-  // one table size for the launch: the largest any job asks for (a job asking
-  // for the default makes it the default)
-  int req = 0;
-  bool any_default = false;
-  for (int j = 0; j < bp.njobs; ++j) {
-    req = std::max(req, bp.job[j].tab_req);
-    any_default = any_default || bp.job[j].tab_req == 0;
-  }
-  constexpr int MINB = min_blocks<MODE, MapT>();
   const int tab_cap = (HAS_QU && any_table) ? table_slots<TabT, MINB>(any_default ? 0 : req) : 0;
   const size_t tab_end = kTabHeaderBytes + align16(sizeof(TabT) * (size_t)tab_cap);
   // one shared region for every job's beam: sized for the largest
@@ -2100,7 +2138,7 @@ int launch_batched(BatchParams& bp, bool any_table, cudaStream_t stream) {
   const int staged = (stage_beam_mode<MODE>() && want_stage && tab_end + stage <= cta_smem_budget<MINB>()) ? 1 : 0;
   const size_t smem = tab_end + (staged ? stage : 0);
   int blocks_per_sm = 0;
-  const int rc = configure_launch<TabT, MINB>(kern, info, mu, smem, blocks_per_sm);
+  const int rc = configure_launch<NT>(kern, info, mu, smem, blocks_per_sm);
   if (rc != TODGPU_OK) return rc;
   for (int j = 0; j < bp.njobs; ++j) {
     bp.job[j].tab_cap = tab_cap;
@@ -2110,10 +2148,27 @@ int launch_batched(BatchParams& bp, bool any_table, cudaStream_t stream) {
   if (T == 0) return TODGPU_OK;
   const long long max_blocks = (long long)sm_count() * blocks_per_sm;
   const int grid = (int)std::max(1LL, std::min(T, max_blocks));
-  kern<<<grid, kNT, smem, stream>>>(bp);
+  kern<<<grid, NT, smem, stream>>>(bp);
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return cuda_fail(e, "gather_batched_kernel launch");
   return TODGPU_OK;
+}
+
+template <int MODE, bool HAS_QU, typename MapT, int PM, int LAYOUT>
+int launch_batched(BatchParams& bp, bool any_table, cudaStream_t stream) {
+  using TabT = typename MapTraits<MapT>::Tab;
+  int req = 0;
+  bool any_default = false, any_wide = false;
+  for (int j = 0; j < bp.njobs; ++j) {
+    req = std::max(req, bp.job[j].tab_req);
+    any_default = any_default || bp.job[j].tab_req == 0;
+    any_wide = any_wide || bp.job[j].flags_wide;
+  }
+  if (!any_wide && !any_default && narrow_fits<TabT>(req))
+    return launch_batched_shape<MODE, HAS_QU, MapT, PM, LAYOUT, kNTNarrow, kMinbNarrow>(bp, any_table, req, false,
+                                                                                        stream);
+  return launch_batched_shape<MODE, HAS_QU, MapT, PM, LAYOUT, kNT, min_blocks<MODE, MapT>()>(bp, any_table, req,
+                                                                                           any_default, stream);
 }
 
 template <int MODE, typename MapT, int PM>

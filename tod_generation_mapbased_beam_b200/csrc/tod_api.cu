@@ -418,6 +418,8 @@ static KArgs make_kargs(const todgpu_gather_args* a) {
   k.tab_req = a->tab_slots;
   k.flags_stage = (a->flags & TODGPU_FLAG_NO_BEAM_STAGE) ? 0 : 1;
   k.beam_stage = 0;
+  k.flags_wide = (a->flags & TODGPU_FLAG_WIDE_CTAS) ? 1 : 0;
+  k.unused = 0;
   return k;
 }
 

@@ -149,12 +149,14 @@ _TABLE_REACH = {}  # data_ptr of a cached ring table -> the reach it was built f
 
 def table_slots(nside, reach):
     """Spin-2 table slots a sample needs for a footprint of radius ``reach``
-    [rad] away from the poles: per window ring the disc's stretch with the
-    kernel's 5% margin and three pixels -- about 1.05 x 3 reach^2 nside^2 for
-    the disc plus 5 per ring over 3 reach nside + 3 rings -- with 10% more
-    and 32 to spare.  Shared memory beyond it is left to L1.  For a reach of
-    0.05 rad or more the kernel reserves whole ring stretches instead of the
-    disc, and the library's default (0) is asked for."""
+    [rad] away from the poles, an upper bound of what the kernel fills (per
+    window ring the disc's stretch, with 2% margin, rounded up): about
+    1.05 x 3 reach^2 nside^2 for the disc plus 5 per ring over 3 reach nside
+    + 3 rings, with 10% more and 32 to spare.  Shared memory beyond it is left
+    to L1, and a request of up to 1438 slots (float64 tables; 2876 float32)
+    lets the launch run 128-thread CTAs, 8 per SM.  For a reach of 0.05 rad or
+    more the kernel reserves whole ring stretches instead of the disc, and the
+    library's default (0) is asked for."""
     r = float(reach)
     n = float(nside)
     if not r < 0.05:

@@ -117,10 +117,15 @@ typedef struct todgpu_gather_args {
   int32_t flags;         /* TODGPU_FLAG_* */
   int32_t tab_slots;     /* spin-2 table slots per sample in shared memory (with a
                             ring table and Q, U): 0 keeps the default of 2048 float64
-                            / 4096 float32 pairs; a footprint's worth (about
-                            3.15 reach^2 nside^2 + 15 reach nside + 15, plus margin)
-                            leaves the rest of the SM's memory to L1.  Capped to what
-                            the kernel's CTAs per SM can share.  Must be >= 0. */
+                            / 4096 float32 pairs and 192 window rings; a footprint's
+                            worth (about 1.05 (3.06 reach^2 nside^2 + 9 reach nside
+                            + 12) + 32) also sizes the window-ring header (for a disc
+                            of tab_slots / 3.2 pixels) and leaves the rest of the
+                            SM's memory to L1; up to about 1500 float64 / 3000
+                            float32 pairs the call runs 128-thread CTAs, 8 per SM.
+                            Capped to what the kernel's CTAs per SM can share.  A
+                            sample whose footprint needs more evaluates its spin-2
+                            angles directly (same results).  Must be >= 0. */
   const void *ring_table;/* optional: table built by todgpu_ring_table_build for this
                             nside; NULL evaluates ring data and spin-2 angles directly */
   const void *theta;     /* (B,) boresight colatitude (TODGPU_ANGLES) */

@@ -1,10 +1,12 @@
 """CPU check of kernels.table_slots: the spin-2 table slots the gather kernel
 fills per sample -- restated here from its footprint setup (window rings of
 the HEALPix RING scheme within reach of the footprint centre, per ring the
-disc's longitude stretch with 5% margin and three pixels, at most the ring
-table's reservation for the table's reach) -- never exceed the request for
-footprint centres anywhere in the disc-sizing range, so no sample loses its
-table to the estimate."""
+disc's longitude stretch with 2% margin rounded up to 2k + 1 slots, at most
+the ring table's reservation for the table's reach) -- never exceed the
+request for footprint centres anywhere in the disc-sizing range, and the
+window's rings never exceed the header the kernel reserves for that request
+(gather_impl.cuh ring_cap_for), so no sample loses its table to the
+estimate."""
 
 import math
 
@@ -54,10 +56,16 @@ def _slots_filled(n, reach_table, reach, theta_u):
                 cnt = min(2 * math.ceil(math.asin(x) / dphi) + 5, npx)
         if disc:
             h2 = reach * reach - (ta - theta_u) ** 2
-            k = math.ceil(1.05 * math.sqrt(h2) / sth / dphi) if h2 > 0 else 0
-            cnt = min(cnt, 2 * k + 3)
+            k = math.ceil(1.02 * math.sqrt(h2) / sth / dphi) if h2 > 0 else 0
+            cnt = min(cnt, 2 * k + 1)
         total += cnt
-    return total
+    return total, ir_hi - ir_lo + 1
+
+
+def _ring_cap_for(requested):
+    """Window rings the kernel's table header holds for a request (restated
+    from gather_impl.cuh ring_cap_for)."""
+    return 192 if requested <= 0 else min(192, math.ceil(3.0 * math.sqrt(requested / 3.2)) + 6)
 
 
 @pytest.mark.parametrize("nside, reach", [(1024, 0.0143), (2048, 0.0146), (512, 0.02), (128, 0.045),
@@ -66,6 +74,8 @@ def test_request_covers_every_footprint(nside, reach):
     reach_table = math.ceil(reach / 1e-4) * 1e-4  # ring tables are built for the reach rounded up
     want = table_slots(nside, reach_table)
     centres = np.linspace(0.1 + reach + 1e-6, math.pi - 0.1 - reach - 1e-6, 601)
-    worst = max(_slots_filled(nside, reach_table, reach, t) for t in centres)
+    filled = [_slots_filled(nside, reach_table, reach, t) for t in centres]
+    worst = max(f[0] for f in filled)
     assert worst <= want
     assert want <= 1.3 * worst + 64  # and not far more (the rest of shared memory is L1)
+    assert max(f[1] for f in filled) <= _ring_cap_for(want)

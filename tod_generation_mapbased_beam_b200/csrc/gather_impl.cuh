@@ -100,7 +100,7 @@ struct KArgs {
   int flags_stage;           // the caller allows staging the beam in shared memory
   int beam_stage;            // the launch made room for the beam in shared memory
   int flags_wide;            // the caller asks for 256-thread CTAs
-  int unused;
+  int ring_cap;              // window rings the launch's table header holds
 };
 
 // Pointing modes of the per-sample rotation.
@@ -455,12 +455,17 @@ struct TableRings {
 // {off, iplo, cap, 0}: slots [off, off + cap) hold cos 2d / sin 2d of its
 // in-ring pixels iplo, iplo + 1, ... (mod n).  hdr = {ir_lo in 32 bits, window
 // rings (0: no table for this sample), filled slots, 0}.
+// A launch reserves ring[0 .. KArgs::ring_cap) (at least 1: ring_win reads
+// ring[0] for a sample without a window; at most kRingCap); the table's slots
+// follow at spin2_header_bytes(ring_cap).
 struct Spin2Tab {
   int4 hdr;
   long long ir_lo;
   long long unused;
   int4 ring[kRingCap];
 };
+static_assert(offsetof(Spin2Tab, ring) == 32 && sizeof(int4) == 16, "Spin2Tab layout");
+__host__ __device__ constexpr size_t spin2_header_bytes(int ring_cap) { return 32 + 16 * (size_t)ring_cap; }
 
 struct Bore {
   double z, sth, phi;
@@ -1667,7 +1672,7 @@ static __device__ __noinline__ void footprint_window(const KArgs& a, const RingR
   ir_hi = min(ir_hi, 4 * a.nside - 1);
   // a non-finite footprint centre gives an empty or invalid window: no table
   const long long nr = ir_hi - ir_lo + 1;
-  bool fits = nr > 0 && nr <= kRingCap && ir_lo >= 1 && ir_hi <= 4 * a.nside - 1;
+  bool fits = nr > 0 && nr <= a.ring_cap && ir_lo >= 1 && ir_hi <= 4 * a.nside - 1;
   // Slots per window ring: the ring's stretch of the footprint disc (radius
   // reach about (theta_u, phi_u)), at most what the ring table reserves
   // for any footprint of that reach.  Away from the poles the disc's
@@ -1743,7 +1748,7 @@ __device__ void run_samples(const KArgs& a, long long t_begin, long long t_end, 
   using TabT = typename MapTraits<MapT>::Tab;
   using Acc = typename std::conditional<MapTraits<MapT>::packed, AccKahan, Acc64>::type;
   using VecT = typename std::conditional<PM == kParamsRef32, float, double>::type;
-  TabT* tab = reinterpret_cast<TabT*>(smem_raw + ((sizeof(Spin2Tab) + 15) & ~size_t(15)));
+  TabT* tab = reinterpret_cast<TabT*>(smem_raw + spin2_header_bytes(a.ring_cap));
   __shared__ SampleBlock s_blk[2];
   __shared__ __align__(8) unsigned long long s_bar;
 
@@ -1774,7 +1779,7 @@ __device__ void run_samples(const KArgs& a, long long t_begin, long long t_end, 
   const float* sbv = nullptr;
   const bool staged = a.beam_stage != 0;
   if (staged) {
-    const size_t off = ((sizeof(Spin2Tab) + 15) & ~size_t(15)) + (((size_t)a.tab_cap * sizeof(TabT) + 15) & ~size_t(15));
+    const size_t off = spin2_header_bytes(a.ring_cap) + (((size_t)a.tab_cap * sizeof(TabT) + 15) & ~size_t(15));
     stage_beam<VecT, NT>(a, smem_raw + off, &s_bar, svec, sbv);
   }
   // one thread derives each sample's rotation and boresight, one sample ahead:
@@ -1987,7 +1992,6 @@ constexpr size_t kSmemPerSM = 228 * 1024;
 constexpr size_t kSmemPerCTAReserved = 1024;
 constexpr size_t kStaticSmemMargin = 2048;
 
-constexpr size_t kTabHeaderBytes = (sizeof(Spin2Tab) + 15) & ~size_t(15);
 #ifndef TODGPU_CTA_THREADS
 #define TODGPU_CTA_THREADS 256
 #endif
@@ -2006,12 +2010,31 @@ constexpr int min_blocks() {
 #endif
 }
 
+// Dynamic shared memory a CTA may take while MINB CTAs still fit on an SM.
+template <int MINB>
+constexpr size_t cta_smem_budget() {
+  return kSmemPerSM / MINB - kSmemPerCTAReserved - kStaticSmemMargin;
+}
+
+// Window rings a launch's table header reserves.  A request of N slots is a
+// footprint disc of at most N / 3.2 pixels (the request of kernels.table_slots
+// is 1.05 x (1.02 x 3 (r nside)^2 + 3 per ring) + 32 for a disc of radius r),
+// so r nside <= sqrt(N / 3.2), and such a disc crosses at most 3 r nside + 4
+// rings of the RING scheme (ring spacing at least 2 / (3 nside) in colatitude,
+// plus the rings either side); the default table reserves kRingCap.  The
+// header then takes 32 + 16 x rings bytes instead of 3 KiB, and the shared
+// memory left goes to L1.
+inline int ring_cap_for(int requested) {
+  if (requested <= 0) return kRingCap;
+  return std::min(kRingCap, (int)std::ceil(3.0 * std::sqrt(requested / 3.2)) + 6);
+}
+
 // Spin-2 table slots of a launch: the caller's request, else 32 KiB (2048
 // float64 or 4096 float32 pairs); never more than each of MINB CTAs can hold
-// in an SM's shared memory.
+// in an SM's shared memory beside the table header.
 template <typename TabT, int MINB>
-constexpr int max_table_slots() {
-  return (int)((kSmemPerSM / MINB - kSmemPerCTAReserved - kStaticSmemMargin - kTabHeaderBytes) / sizeof(TabT));
+int max_table_slots(int ring_cap) {
+  return (int)((cta_smem_budget<MINB>() - spin2_header_bytes(ring_cap)) / sizeof(TabT));
 }
 constexpr size_t align16(size_t x) { return (x + 15) & ~size_t(15); }
 
@@ -2023,16 +2046,10 @@ constexpr bool stage_beam_mode() {
   return MODE == TODGPU_BILINEAR;
 }
 
-// Dynamic shared memory a CTA may take while MINB CTAs still fit on an SM.
-template <int MINB>
-constexpr size_t cta_smem_budget() {
-  return kSmemPerSM / MINB - kSmemPerCTAReserved - kStaticSmemMargin;
-}
-
 template <typename TabT, int MINB>
 int table_slots(int requested) {
   constexpr int kCap = (int)(kTabCapDefault * sizeof(double2) / sizeof(TabT));
-  return requested > 0 ? std::min(requested, max_table_slots<TabT, MINB>()) : kCap;
+  return requested > 0 ? std::min(requested, max_table_slots<TabT, MINB>(ring_cap_for(requested))) : kCap;
 }
 
 // Once per kernel: allow the largest table; per launch: CTAs per SM for the
@@ -2078,8 +2095,8 @@ constexpr int kNTNarrow = 128;
 constexpr int kMinbNarrow = 8;
 
 template <typename TabT>
-constexpr bool narrow_fits(int requested) {
-  return requested > 0 && requested <= max_table_slots<TabT, kMinbNarrow>();
+bool narrow_fits(int requested) {
+  return requested > 0 && requested <= max_table_slots<TabT, kMinbNarrow>(ring_cap_for(requested));
 }
 
 template <int MODE, bool HAS_QU, typename MapT, int PM, int LAYOUT, int NT, int MINB>
@@ -2088,8 +2105,10 @@ int launch_gather_shape(KArgs k, cudaStream_t stream) {
   static LaunchInfo info;
   static std::mutex mu;
   using TabT = typename MapTraits<MapT>::Tab;
-  const int tab_cap = (HAS_QU && k.ring_table != nullptr) ? table_slots<TabT, MINB>(k.tab_req) : 0;
-  const size_t tab_end = kTabHeaderBytes + align16(sizeof(TabT) * (size_t)tab_cap);
+  const bool tab = HAS_QU && k.ring_table != nullptr;
+  const int tab_cap = tab ? table_slots<TabT, MINB>(k.tab_req) : 0;
+  k.ring_cap = tab ? ring_cap_for(k.tab_req) : 1;  // ring[0] is read (not used) without a window
+  const size_t tab_end = spin2_header_bytes(k.ring_cap) + align16(sizeof(TabT) * (size_t)tab_cap);
   const size_t stage = beam_stage_bytes(k.S, PM == kParamsRef32 ? sizeof(float) : sizeof(double));
   k.beam_stage = (stage_beam_mode<MODE>() && k.flags_stage && tab_end + stage <= cta_smem_budget<MINB>()) ? 1 : 0;
   const size_t smem = tab_end + (k.beam_stage ? stage : 0);
@@ -2127,7 +2146,8 @@ int launch_batched_shape(BatchParams& bp, bool any_table, int req, bool any_defa
   static std::mutex mu;
   using TabT = typename MapTraits<MapT>::Tab;
   const int tab_cap = (HAS_QU && any_table) ? table_slots<TabT, MINB>(any_default ? 0 : req) : 0;
-  const size_t tab_end = kTabHeaderBytes + align16(sizeof(TabT) * (size_t)tab_cap);
+  const int ring_cap = (HAS_QU && any_table) ? ring_cap_for(any_default ? 0 : req) : 1;
+  const size_t tab_end = spin2_header_bytes(ring_cap) + align16(sizeof(TabT) * (size_t)tab_cap);
   // one shared region for every job's beam: sized for the largest
   size_t stage = 0;
   bool want_stage = true;
@@ -2142,6 +2162,7 @@ int launch_batched_shape(BatchParams& bp, bool any_table, int req, bool any_defa
   if (rc != TODGPU_OK) return rc;
   for (int j = 0; j < bp.njobs; ++j) {
     bp.job[j].tab_cap = tab_cap;
+    bp.job[j].ring_cap = ring_cap;
     bp.job[j].beam_stage = staged;
   }
   const long long T = bp.tiles_before[bp.njobs];

@@ -419,7 +419,7 @@ static KArgs make_kargs(const todgpu_gather_args* a) {
   k.flags_stage = (a->flags & TODGPU_FLAG_NO_BEAM_STAGE) ? 0 : 1;
   k.beam_stage = 0;
   k.flags_wide = (a->flags & TODGPU_FLAG_WIDE_CTAS) ? 1 : 0;
-  k.unused = 0;
+  k.ring_cap = 0;
   return k;
 }
 

@@ -149,20 +149,23 @@ _TABLE_REACH = {}  # data_ptr of a cached ring table -> the reach it was built f
 
 def table_slots(nside, reach):
     """Spin-2 table slots a sample needs for a footprint of radius ``reach``
-    [rad] away from the poles, an upper bound of what the kernel fills (per
-    window ring the disc's stretch, with 2% margin, rounded up): about
-    1.05 x 3 reach^2 nside^2 for the disc plus 5 per ring over 3 reach nside
-    + 3 rings, with 10% more and 32 to spare.  Shared memory beyond it is left
-    to L1, and a request of up to 1438 slots (float64 tables; 2876 float32)
-    lets the launch run 128-thread CTAs, 8 per SM.  For a reach of 0.05 rad or
-    more the kernel reserves whole ring stretches instead of the disc, and the
+    [rad] away from the poles, an upper bound of what the kernel fills: per
+    window ring the disc's stretch with 2% margin, rounded up to 2k + 1 slots
+    -- at most 1.02 x 3 (reach nside)^2 for the disc plus 3 per ring over at
+    most 3 reach nside + 4 rings -- with 5% more and 32 to spare.  The request
+    also sizes the table header (the kernel reserves window rings for a disc
+    of request / 3.2 pixels).  Shared memory beyond them is left to L1, and a
+    request of up to about 1500 slots (float64 tables; 3000 float32) lets the
+    launch run 128-thread CTAs, 8 per SM.  For a reach of 0.05 rad or more the
+    kernel reserves whole ring stretches instead of the disc, and the
     library's default (0) is asked for."""
     r = float(reach)
     n = float(nside)
     if not r < 0.05:
         return 0
-    need = 1.05 * 3.0 * r * r * n * n + 5.0 * (3.0 * r * n + 3.0)
-    return int(min(1 << 20, math.ceil(1.1 * need) + 32))
+    x = r * n
+    need = 1.02 * 3.0 * x * x + 3.0 * (3.0 * x + 4.0)
+    return int(min(1 << 20, math.ceil(1.05 * need) + 32))
 
 
 def table_slots_for(table, nside):

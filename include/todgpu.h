@@ -120,9 +120,10 @@ typedef struct todgpu_gather_args {
                             / 4096 float32 pairs and 192 window rings; a footprint's
                             worth (about 1.05 (3.06 reach^2 nside^2 + 9 reach nside
                             + 12) + 32) also sizes the window-ring header (for a disc
-                            of tab_slots / 3.2 pixels) and leaves the rest of the
-                            SM's memory to L1; up to about 1500 float64 / 3000
-                            float32 pairs the call runs 128-thread CTAs, 8 per SM.
+                            of tab_slots / 3.2 pixels; 128-thread CTAs reserve 80
+                            rings) and leaves the rest of the SM's memory to L1; up
+                            to about 1500 float64 / 3000 float32 pairs the call runs
+                            128-thread CTAs, 8 per SM.
                             Capped to what the kernel's CTAs per SM can share.  A
                             sample whose footprint needs more evaluates its spin-2
                             angles directly (same results).  Must be >= 0. */

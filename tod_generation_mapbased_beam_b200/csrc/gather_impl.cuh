@@ -58,6 +58,12 @@ constexpr int kNTStatic = 256;  // threads of the reach kernel of the built-in t
 // order), whatever the CTA's thread count, so CTAs of 128 and 256 threads
 // give the same TOD bit for bit.
 constexpr int kSumLanes = 256;
+// The narrow CTA shape (128 threads, 8 per SM) and the window rings its table
+// header always reserves, so that the table's offset is a compile-time constant
+// of that shape (the wide shape sizes its header per launch).
+constexpr int kNTNarrow = 128;
+constexpr int kMinbNarrow = 8;
+constexpr int kRingCapNarrow = 80;
 
 // Message of the calling thread's last failure (defined in tod_api.cu).
 extern thread_local std::string g_last_error;
@@ -1748,7 +1754,9 @@ __device__ void run_samples(const KArgs& a, long long t_begin, long long t_end, 
   using TabT = typename MapTraits<MapT>::Tab;
   using Acc = typename std::conditional<MapTraits<MapT>::packed, AccKahan, Acc64>::type;
   using VecT = typename std::conditional<PM == kParamsRef32, float, double>::type;
-  TabT* tab = reinterpret_cast<TabT*>(smem_raw + spin2_header_bytes(a.ring_cap));
+  // window rings of the table header (a.ring_cap; a constant in the narrow shape)
+  const int hdr_rings = NT == kNTNarrow ? kRingCapNarrow : a.ring_cap;
+  TabT* tab = reinterpret_cast<TabT*>(smem_raw + spin2_header_bytes(hdr_rings));
   __shared__ SampleBlock s_blk[2];
   __shared__ __align__(8) unsigned long long s_bar;
 
@@ -1779,7 +1787,7 @@ __device__ void run_samples(const KArgs& a, long long t_begin, long long t_end, 
   const float* sbv = nullptr;
   const bool staged = a.beam_stage != 0;
   if (staged) {
-    const size_t off = spin2_header_bytes(a.ring_cap) + (((size_t)a.tab_cap * sizeof(TabT) + 15) & ~size_t(15));
+    const size_t off = spin2_header_bytes(hdr_rings) + (((size_t)a.tab_cap * sizeof(TabT) + 15) & ~size_t(15));
     stage_beam<VecT, NT>(a, smem_raw + off, &s_bar, svec, sbv);
   }
   // one thread derives each sample's rotation and boresight, one sample ahead:
@@ -2047,9 +2055,16 @@ constexpr bool stage_beam_mode() {
 }
 
 template <typename TabT, int MINB>
-int table_slots(int requested) {
+int table_slots(int requested, int ring_cap) {
   constexpr int kCap = (int)(kTabCapDefault * sizeof(double2) / sizeof(TabT));
-  return requested > 0 ? std::min(requested, max_table_slots<TabT, MINB>(ring_cap_for(requested))) : kCap;
+  return requested > 0 ? std::min(requested, max_table_slots<TabT, MINB>(ring_cap)) : kCap;
+}
+
+// Window rings of a launch's table header: fixed in the narrow shape.
+template <int NT>
+int header_rings(bool table, int requested) {
+  if (NT == kNTNarrow) return kRingCapNarrow;
+  return table ? ring_cap_for(requested) : 1;  // ring[0] is read (not used) without a window
 }
 
 // Once per kernel: allow the largest table; per launch: CTAs per SM for the
@@ -2091,12 +2106,10 @@ int configure_launch(Kern kern, LaunchInfo& info, std::mutex& mu, size_t smem, i
 // 3.3k slots) keep the wide shape: in the narrow one their tables would not fit
 // and their samples would fall back to direct spin-2 evaluation.  The TOD is
 // the same bit for bit in either shape (kSumLanes).
-constexpr int kNTNarrow = 128;
-constexpr int kMinbNarrow = 8;
-
 template <typename TabT>
 bool narrow_fits(int requested) {
-  return requested > 0 && requested <= max_table_slots<TabT, kMinbNarrow>(ring_cap_for(requested));
+  return requested > 0 && ring_cap_for(requested) <= kRingCapNarrow &&
+         requested <= max_table_slots<TabT, kMinbNarrow>(kRingCapNarrow);
 }
 
 template <int MODE, bool HAS_QU, typename MapT, int PM, int LAYOUT, int NT, int MINB>
@@ -2106,8 +2119,8 @@ int launch_gather_shape(KArgs k, cudaStream_t stream) {
   static std::mutex mu;
   using TabT = typename MapTraits<MapT>::Tab;
   const bool tab = HAS_QU && k.ring_table != nullptr;
-  const int tab_cap = tab ? table_slots<TabT, MINB>(k.tab_req) : 0;
-  k.ring_cap = tab ? ring_cap_for(k.tab_req) : 1;  // ring[0] is read (not used) without a window
+  k.ring_cap = header_rings<NT>(tab, k.tab_req);
+  const int tab_cap = tab ? table_slots<TabT, MINB>(k.tab_req, k.ring_cap) : 0;
   const size_t tab_end = spin2_header_bytes(k.ring_cap) + align16(sizeof(TabT) * (size_t)tab_cap);
   const size_t stage = beam_stage_bytes(k.S, PM == kParamsRef32 ? sizeof(float) : sizeof(double));
   k.beam_stage = (stage_beam_mode<MODE>() && k.flags_stage && tab_end + stage <= cta_smem_budget<MINB>()) ? 1 : 0;
@@ -2145,8 +2158,8 @@ int launch_batched_shape(BatchParams& bp, bool any_table, int req, bool any_defa
   static LaunchInfo info;
   static std::mutex mu;
   using TabT = typename MapTraits<MapT>::Tab;
-  const int tab_cap = (HAS_QU && any_table) ? table_slots<TabT, MINB>(any_default ? 0 : req) : 0;
-  const int ring_cap = (HAS_QU && any_table) ? ring_cap_for(any_default ? 0 : req) : 1;
+  const int ring_cap = header_rings<NT>(HAS_QU && any_table, any_default ? 0 : req);
+  const int tab_cap = (HAS_QU && any_table) ? table_slots<TabT, MINB>(any_default ? 0 : req, ring_cap) : 0;
   const size_t tab_end = spin2_header_bytes(ring_cap) + align16(sizeof(TabT) * (size_t)tab_cap);
   // one shared region for every job's beam: sized for the largest
   size_t stage = 0;

@@ -153,8 +153,8 @@ def table_slots(nside, reach):
     window ring the disc's stretch with 2% margin, rounded up to 2k + 1 slots
     -- at most 1.02 x 3 (reach nside)^2 for the disc plus 3 per ring over at
     most 3 reach nside + 4 rings -- with 5% more and 32 to spare.  The request
-    also sizes the table header (the kernel reserves window rings for a disc
-    of request / 3.2 pixels).  Shared memory beyond them is left to L1, and a
+    also sizes the table header (256-thread CTAs reserve window rings for a
+    disc of request / 3.2 pixels, 128-thread CTAs a fixed 80).  Shared memory beyond them is left to L1, and a
     request of up to about 1500 slots (float64 tables; 3000 float32) lets the
     launch run 128-thread CTAs, 8 per SM.  For a reach of 0.05 rad or more the
     kernel reserves whole ring stretches instead of the disc, and the

@@ -2047,8 +2047,9 @@ int max_table_slots(int ring_cap) {
 constexpr size_t align16(size_t x) { return (x + 15) & ~size_t(15); }
 
 // Modes whose launches stage the beam in shared memory when it fits: bilinear
-// (config 2: +5%); nearest reads one stencil pixel per beam pixel and gains
-// more from the shared memory left to L1 (config 2: 1% faster without).
+// (config 2 in 256-thread CTAs: +5%; its 128-thread CTAs have no room for
+// the beam beside the table); nearest reads one stencil pixel per beam pixel
+// and gains more from the shared memory left to L1 (1% faster without).
 template <int MODE>
 constexpr bool stage_beam_mode() {
   return MODE == TODGPU_BILINEAR;

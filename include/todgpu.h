@@ -122,7 +122,7 @@ typedef struct todgpu_gather_args {
                             + 12) + 32) also sizes the window-ring header (for a disc
                             of tab_slots / 3.2 pixels; 128-thread CTAs reserve 80
                             rings) and leaves the rest of the SM's memory to L1; up
-                            to about 1500 float64 / 3000 float32 pairs the call runs
+                            to about 1500 float64 / 1900 float32 pairs the call runs
                             128-thread CTAs, 8 per SM.
                             Capped to what the kernel's CTAs per SM can share.  A
                             sample whose footprint needs more evaluates its spin-2

@@ -7,6 +7,8 @@ same 256 strided partial sums, reduced in the same order, so the TOD must not
 change: for both interpolation modes, every map type, the three pointing forms,
 beams of a few pixels and beams too large to stage, and the batched launch."""
 
+import math
+
 import numpy as np
 import pytest
 import torch
@@ -20,9 +22,14 @@ from tod_generation_mapbased_beam_b200.kernels import (beam_reach, gather_accum,
 pytestmark = pytest.mark.gpu
 
 # spin-2 table slots of a 128-thread CTA at 8 per SM: (228 KiB / 8 - 3 KiB
-# reserved - 3104 B table header) / 16 B per float64 pair
-NARROW_F64_SLOTS = (228 * 1024 // 8 - 1024 - 2048 - 3104) // 16
+# reserved - 1312 B table header of 80 window rings) / 16 B per float64 pair;
+# the request must also need at most those 80 rings (3 sqrt(slots / 3.2) + 6)
+NARROW_F64_SLOTS = (228 * 1024 // 8 - 1024 - 2048 - (32 + 16 * 80)) // 16
 WIDE = _native.FLAG_WIDE_CTAS
+
+
+def _narrow(slots):
+    return 0 < slots <= NARROW_F64_SLOTS and math.ceil(3.0 * math.sqrt(slots / 3.2)) + 6 <= 80
 
 
 def _beam(S, seed, radius_deg=0.7):
@@ -55,7 +62,7 @@ def test_narrow_shape_is_taken():
     launches would be wide and the comparison empty)."""
     for nside, S in ((512, 900), (256, 1300)):
         vec, _ = _beam(S, 3)
-        assert 0 < table_slots(nside, beam_reach(vec.astype(np.float32), nside)) <= NARROW_F64_SLOTS
+        assert _narrow(table_slots(nside, beam_reach(vec.astype(np.float32), nside)))
 
 
 @pytest.mark.parametrize("interp", [_native.BILINEAR, _native.NEAREST])

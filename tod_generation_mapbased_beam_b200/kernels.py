@@ -155,7 +155,7 @@ def table_slots(nside, reach):
     most 3 reach nside + 4 rings -- with 5% more and 32 to spare.  The request
     also sizes the table header (256-thread CTAs reserve window rings for a
     disc of request / 3.2 pixels, 128-thread CTAs a fixed 80).  Shared memory beyond them is left to L1, and a
-    request of up to about 1500 slots (float64 tables; 3000 float32) lets the
+    request of up to about 1500 slots (float64 tables; 1900 float32) lets the
     launch run 128-thread CTAs, 8 per SM.  For a reach of 0.05 rad or more the
     kernel reserves whole ring stretches instead of the disc, and the
     library's default (0) is asked for."""

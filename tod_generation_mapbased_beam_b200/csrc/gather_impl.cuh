@@ -2100,13 +2100,14 @@ int configure_launch(Kern kern, LaunchInfo& info, std::mutex& mu, size_t smem, i
 // Two CTA shapes.  Wide: kNT (256) threads, min_blocks() CTAs per SM, room
 // for the default 32 KiB spin-2 table and the staged beam.  Narrow: 128
 // threads, 8 CTAs per SM at 64 registers, for launches whose requested table
-// fits an eighth of an SM's shared memory (config 2: 1.1k slots of 16 B): with
-// twice the CTAs per SM, the per-sample setup and barriers of one CTA overlap
-// the pixel loops of more others (config 2 bilinear +12%, nearest +7%, although
-// the beam no longer fits beside the table).  Larger footprints (config 3:
-// 3.3k slots) keep the wide shape: in the narrow one their tables would not fit
-// and their samples would fall back to direct spin-2 evaluation.  The TOD is
-// the same bit for bit in either shape (kSumLanes).
+// fits an eighth of an SM's shared memory beside the shape's 80-ring header
+// (config 2: 820 slots of 16 B): with more CTAs per SM, the per-sample setup
+// and barriers of one CTA overlap the pixel loops of more others (config 2
+// bilinear +12%, nearest +7%, although the beam no longer fits beside the
+// table).  Larger footprints (config 3: 3.2k slots) keep the wide shape: in
+// the narrow one their tables would not fit and their samples would fall back
+// to direct spin-2 evaluation.  The TOD is the same bit for bit in either
+// shape (kSumLanes).
 template <typename TabT>
 bool narrow_fits(int requested) {
   return requested > 0 && ring_cap_for(requested) <= kRingCapNarrow &&
